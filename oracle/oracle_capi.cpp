@@ -1,0 +1,137 @@
+// ORACLE — test infrastructure only. C entry points of the CPU restatement,
+// loaded with ctypes by tests/ and bench.py (CPU baseline); never by the
+// product library.
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "edlib_nw.hpp"
+#include "racon_cpu.hpp"
+
+using namespace oracle;
+
+extern "C" {
+
+// NW edit distance only (test/racon_test.cpp:16-25 metric).
+int oracle_nw_distance(const char* q, int qlen, const char* t, int tlen) {
+    return nw_align(q, qlen, t, tlen, false).edit_distance;
+}
+
+// NW with path (src/overlap.cpp:205-224). Writes the standard CIGAR into
+// cigar[0..cap) (NUL-terminated when it fits) and its length to *cigar_len.
+// Returns the edit distance, or -1 on failure.
+int oracle_nw_cigar(const char* q, int qlen, const char* t, int tlen, char* cigar,
+                    int cap, int* cigar_len) {
+    NwResult r = nw_align(q, qlen, t, tlen, true);
+    if (!r.ok) return -1;
+    const std::string c = ops_to_cigar(r.ops);
+    *cigar_len = int(c.size());
+    if (int(c.size()) < cap) memcpy(cigar, c.c_str(), c.size() + 1);
+    return r.edit_distance;
+}
+
+// Breaking points from a CIGAR (src/overlap.cpp:226-292); writes
+// (t,q) pairs as 2*count uint32 values; returns the number of values, or the
+// negative required size when cap is too small.
+int oracle_breakpoints(const char* cigar, uint32_t q_begin, uint32_t q_end,
+                       uint32_t q_length, uint32_t t_begin, uint32_t t_end,
+                       uint32_t strand, uint32_t window_length, uint32_t* out, int cap) {
+    CpuOverlap o;
+    o.cigar = cigar;
+    o.q_begin = q_begin;
+    o.q_end = q_end;
+    o.q_length = q_length;
+    o.t_begin = t_begin;
+    o.t_end = t_end;
+    o.strand = strand;
+    std::vector<std::pair<uint32_t, uint32_t>> bp;
+    breakpoints_from_cigar(o, window_length, bp);
+    const int need = int(bp.size() * 2);
+    if (need > cap) return -need;
+    for (size_t i = 0; i < bp.size(); ++i) {
+        out[2 * i] = bp[i].first;
+        out[2 * i + 1] = bp[i].second;
+    }
+    return need;
+}
+
+// Window::generate_consensus (src/window.cpp:65-142) on one window. quals[i]
+// may be NULL. Returns 1 when polished, 0 when the backbone was kept, -1 when
+// cap is too small (out_len then holds the size needed).
+int oracle_window_consensus(const char* backbone, const char* bqual, uint32_t blen,
+                            uint32_t nlayers, const char* const* seqs,
+                            const char* const* quals, const uint32_t* lens,
+                            const uint32_t* begins, const uint32_t* ends, int tgs, int trim,
+                            int match, int mismatch, int gap, char* out, int cap,
+                            int* out_len, uint64_t* cells_out, uint32_t* nodes_out) {
+    CpuWindowInput w;
+    w.backbone = backbone;
+    w.backbone_len = blen;
+    w.backbone_qual = bqual;
+    for (uint32_t i = 0; i < nlayers; ++i) {
+        w.seqs.push_back(seqs[i]);
+        w.quals.push_back(quals ? quals[i] : nullptr);
+        w.lens.push_back(lens[i]);
+        w.positions.emplace_back(begins[i], ends[i]);
+    }
+    std::string cons;
+    WindowStats st;
+    const bool pol = window_consensus(w, tgs != 0, trim != 0, match, mismatch, gap, cons, &st);
+    if (cells_out) *cells_out = st.cells;
+    if (nodes_out) *nodes_out = st.nodes;
+    *out_len = int(cons.size());
+    if (int(cons.size()) > cap) return -1;
+    memcpy(out, cons.data(), cons.size());
+    return pol ? 1 : 0;
+}
+
+// Full pipeline; returns a malloc'd FASTA text (free with oracle_free), or
+// NULL where racon would exit(1). times[0..4] = load, align, layers,
+// consensus seconds; counts[0..2] = overlaps, windows, poa cells.
+char* oracle_polish(const char* sequences, const char* overlaps, const char* targets,
+                    int fragment, uint32_t window_length, double quality_threshold,
+                    double error_threshold, int trim, int match, int mismatch, int gap,
+                    uint32_t threads, int drop_unpolished, double* times, uint64_t* counts) {
+    PolishOptions opt;
+    opt.fragment = fragment != 0;
+    opt.window_length = window_length;
+    opt.quality_threshold = quality_threshold;
+    opt.error_threshold = error_threshold;
+    opt.trim = trim != 0;
+    opt.match = match;
+    opt.mismatch = mismatch;
+    opt.gap = gap;
+    opt.threads = threads;
+    opt.drop_unpolished = drop_unpolished != 0;
+    std::vector<std::pair<std::string, std::string>> out;
+    PolishTimes tm;
+    if (polish_files(sequences, overlaps, targets, opt, out, &tm)) return nullptr;
+    if (times) {
+        times[0] = tm.load_s;
+        times[1] = tm.align_s;
+        times[2] = tm.layers_s;
+        times[3] = tm.consensus_s;
+    }
+    if (counts) {
+        counts[0] = tm.overlaps;
+        counts[1] = tm.windows;
+        counts[2] = tm.poa_cells;
+    }
+    std::string text;
+    for (const auto& s : out) {
+        text += '>';
+        text += s.first;
+        text += '\n';
+        text += s.second;
+        text += '\n';
+    }
+    char* buf = static_cast<char*>(malloc(text.size() + 1));
+    memcpy(buf, text.c_str(), text.size() + 1);
+    return buf;
+}
+
+void oracle_free(void* p) { free(p); }
+
+}  // extern "C"
