@@ -1,0 +1,209 @@
+/*
+ * racon_b200 — C ABI of the B200 polishing hot path.
+ *
+ * The library replaces the two third-party calls on racon's polishing path:
+ *   - per-overlap global alignment + window breaking points
+ *       racon src/overlap.cpp:179-203 (Overlap::find_breaking_points),
+ *       :205-224 (Overlap::align_overlaps: edlibAlign NW + standard CIGAR),
+ *       :226-292 (Overlap::find_breaking_points_from_cigar),
+ *     driven from src/polisher.cpp:462-484 (Polisher::find_overlap_breaking_points);
+ *   - per-window partial-order consensus
+ *       racon src/window.cpp:65-142 (Window::generate_consensus),
+ *     driven from src/polisher.cpp:486-504 (Polisher::polish).
+ * In the reference these two seams are the virtual methods that the CUDA
+ * plug-in overrides (src/cuda/cudapolisher.hpp:23-24, :43); the C++ host layer
+ * of this project (racon_b200/csrc/host) overrides the same two methods and
+ * calls the functions below. Inputs are host pointers plus lengths; the
+ * library copies them to the device, so nothing here keeps pointers to caller
+ * memory after a call returns. Results live in library-owned buffers that stay
+ * valid until the next call of the same kind on the same context or
+ * rb_destroy().
+ *
+ * Every function returns RB_OK (0) or a nonzero RB_ERR_* code; the message is
+ * in rb_last_error(). There is no CPU fallback: a failing device step is an
+ * error, never a silent host computation.
+ */
+#ifndef RACON_B200_H_
+#define RACON_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RB_OK 0
+#define RB_ERR_ARG 1      /* invalid argument or input outside documented limits */
+#define RB_ERR_CUDA 2     /* CUDA runtime error */
+#define RB_ERR_NOMEM 3    /* device or pinned host allocation failed */
+#define RB_ERR_DEVICE 4   /* a kernel reported a failure status */
+#define RB_ERR_NODEV 5    /* no usable sm_100 device */
+
+typedef struct rb_ctx rb_ctx;
+
+/* Scoring and windowing of one polishing job: racon's -m -x -g -w
+ * (src/main.cpp:51-67, passed to createPolisher, src/polisher.hpp:42-48). */
+typedef struct rb_params {
+    int8_t match;
+    int8_t mismatch;
+    int8_t gap;
+    uint32_t window_length;
+} rb_params;
+
+/* Creates a context on CUDA device `device`. Replaces the per-device set-up of
+ * the reference plug-in (src/cuda/cudapolisher.cpp:27-66). Returns NULL on
+ * failure; rb_create_error() then holds the reason. */
+rb_ctx* rb_create(int device, const rb_params* params);
+const char* rb_create_error(void);
+void rb_destroy(rb_ctx* ctx);
+const char* rb_last_error(const rb_ctx* ctx);
+
+/* ---------------------------------------------------------------------
+ * Overlap alignment (replaces src/overlap.cpp:179-292 per overlap)
+ * ------------------------------------------------------------------- */
+
+/* One overlap, already cut to its aligned spans (src/overlap.cpp:193-197):
+ * query = read span, reverse-complemented for '-' strand; target = contig
+ * span. q_offset is the read coordinate of query[0] in the orientation used
+ * (strand ? q_length - q_end : q_begin, src/overlap.cpp:241); t_begin is the
+ * target coordinate of target[0]. Spans are limited to 2^24 bases. */
+typedef struct rb_pair {
+    const char* query;
+    uint32_t query_length;
+    const char* target;
+    uint32_t target_length;
+    uint32_t q_offset;
+    uint32_t t_begin;
+} rb_pair;
+
+/* Results of rb_align_batch, library-owned. breakpoints holds, for pair i,
+ * the (t, q) uint32 pairs breakpoints[bp_offsets[i] .. bp_offsets[i+1]) in
+ * racon's order (first match, last match + 1 per window,
+ * src/overlap.cpp:259-266). cigars holds the standard CIGAR of pair i at
+ * cigars[cigar_offsets[i] .. cigar_offsets[i+1]) (not NUL-terminated) when
+ * want_cigar was set, else cigars/cigar_offsets are NULL. */
+typedef struct rb_aln_result {
+    const int32_t* edit_distance;
+    const uint32_t* breakpoints;
+    const uint64_t* bp_offsets;
+    const char* cigars;
+    const uint64_t* cigar_offsets;
+} rb_aln_result;
+
+/* Aligns n pairs on the device (edlib NW + path semantics, k doubling from 64,
+ * Hirschberg above 1 MiB of traceback data) and derives the window breaking
+ * points for window_length from rb_params. */
+int rb_align_batch(rb_ctx* ctx, const rb_pair* pairs, size_t n, int want_cigar,
+                   rb_aln_result* out);
+
+/* ---------------------------------------------------------------------
+ * Window consensus (replaces src/window.cpp:65-142 per window)
+ * ------------------------------------------------------------------- */
+
+/* One window: the backbone (target slice) and its layers as racon's
+ * Window::add_layer stored them (src/window.cpp:42-63). backbone_quality may
+ * be NULL (weight 0 everywhere, racon's dummy '!' quality,
+ * src/polisher.cpp:171, :393-395). layer_qualities may be NULL or hold NULL
+ * entries (weight 1 per base). begins/ends are backbone coordinates. tgs is 1
+ * for racon's WindowType::kTGS (mean read length > 1000,
+ * src/polisher.cpp:276-277). id and rank only label the chimeric-window
+ * warning (src/window.cpp:133-135). Limits: backbone_length <= 65535,
+ * n_layers <= 65535, layer_length <= 65535, begin < end < backbone_length
+ * (racon's layers always end on a backbone base). */
+typedef struct rb_window {
+    const char* backbone;
+    const char* backbone_quality;
+    uint32_t backbone_length;
+    uint32_t n_layers;
+    const char* const* layers;
+    const char* const* layer_qualities;
+    const uint32_t* layer_lengths;
+    const uint32_t* begins;
+    const uint32_t* ends;
+    uint8_t tgs;
+    uint64_t id;
+    uint32_t rank;
+} rb_window;
+
+/* Consensus of window i at consensus[offsets[i] .. offsets[i+1]);
+ * polished[i] is 1 when the window had at least two layers (the return value
+ * of Window::generate_consensus), else 0 and the consensus is the backbone. */
+typedef struct rb_poa_result {
+    const char* consensus;
+    const uint64_t* offsets;
+    const uint8_t* polished;
+} rb_poa_result;
+
+/* Computes the consensus of n windows on the device; trim is racon's
+ * --no-trimming negation (src/window.cpp:118-139). */
+int rb_poa_batch(rb_ctx* ctx, const rb_window* windows, size_t n, int trim,
+                 rb_poa_result* out);
+
+/* Device-resident form of rb_poa_batch for throughput measurement: stage
+ * packs and copies the windows to the device once, run computes the
+ * consensus of every staged window with inputs and outputs already in device
+ * memory, fetch copies the results back. rb_poa_batch == stage + run + fetch. */
+int rb_poa_stage(rb_ctx* ctx, const rb_window* windows, size_t n, int trim);
+int rb_poa_run(rb_ctx* ctx);
+int rb_poa_fetch(rb_ctx* ctx, rb_poa_result* out);
+
+/* Breaking points of overlaps that already carry an alignment (SAM input:
+ * src/overlap.cpp:192-200 skips the aligner when the CIGAR is set and walks
+ * it in find_breaking_points_from_cigar, :226-292). cigar is the SAM CIGAR
+ * (M, =, X, I, D, N, S, H, P); q_offset is the read coordinate before the
+ * first aligned base in the orientation used (strand ? q_length - q_end :
+ * q_begin); the alignment covers target [t_begin, t_end). Results use
+ * rb_aln_result with edit_distance entries set to -1 and no CIGARs. */
+typedef struct rb_cigar_overlap {
+    const char* cigar;
+    uint32_t cigar_length;
+    uint32_t q_offset;
+    uint32_t t_begin;
+    uint32_t t_end;
+} rb_cigar_overlap;
+int rb_cigar_breakpoints(rb_ctx* ctx, const rb_cigar_overlap* overlaps, size_t n,
+                         rb_aln_result* out);
+
+/* Same split for the overlap aligner. */
+int rb_align_stage(rb_ctx* ctx, const rb_pair* pairs, size_t n, int want_cigar);
+int rb_align_run(rb_ctx* ctx);
+int rb_align_fetch(rb_ctx* ctx, rb_aln_result* out);
+
+/* Counters of the last run/batch call of each kind. */
+typedef struct rb_stats {
+    double kernel_ms;        /* device time of the compute kernels (CUDA events) */
+    double h2d_ms, d2h_ms;   /* copy time of the last batch call */
+    uint64_t h2d_bytes, d2h_bytes;
+    uint64_t launches;       /* kernels launched by the last run */
+    uint64_t cells;          /* DP cells (POA: |layer| x |aligned graph|) */
+    uint64_t items;          /* windows or pairs processed */
+    uint32_t max_nodes;      /* POA: largest graph seen */
+    double top_kernel_ms;    /* device time of the dominant kernel */
+} rb_stats;
+int rb_poa_stats(const rb_ctx* ctx, rb_stats* out);
+int rb_align_stats(const rb_ctx* ctx, rb_stats* out);
+
+/* ---------------------------------------------------------------------
+ * Whole pipeline (createPolisher + initialize + polish, src/main.cpp:152-166)
+ * ------------------------------------------------------------------- */
+
+/* Runs racon's pipeline with the device hot path and returns the polished
+ * FASTA text (">name tags\nsequence\n" records) in *fasta, allocated with
+ * malloc (free with rb_free). fragment = -f, drop_unpolished = !-u.
+ * On input errors racon prints "[racon::...] error: ..." and exits(1); this
+ * entry point returns RB_ERR_ARG with the same message in rb_pipeline_error().
+ * device selects the CUDA device; threads is accepted for -t compatibility. */
+int rb_polish_files(const char* sequences_path, const char* overlaps_path,
+                    const char* target_path, int fragment, uint32_t window_length,
+                    double quality_threshold, double error_threshold, int trim,
+                    int8_t match, int8_t mismatch, int8_t gap, uint32_t threads,
+                    int drop_unpolished, int device, char** fasta, double* stage_seconds);
+const char* rb_pipeline_error(void);
+void rb_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RACON_B200_H_ */

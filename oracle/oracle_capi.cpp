@@ -135,3 +135,55 @@ char* oracle_polish(const char* sequences, const char* overlaps, const char* tar
 void oracle_free(void* p) { free(p); }
 
 }  // extern "C"
+
+extern "C" {
+
+// Every window after initialize() (src/polisher.cpp:192-460) as a binary blob
+// (free with oracle_free). Layout, little endian, per window:
+//   u64 target_id, u32 rank, u8 tgs, u32 backbone_len, u32 n_layers,
+//   backbone bytes, backbone quality bytes,
+//   per layer: u32 len, u32 begin, u32 end, u8 has_quality, bytes, [quality]
+// preceded by a u64 window count. Returns NULL on error.
+char* oracle_dump_windows(const char* sequences, const char* overlaps, const char* targets,
+                          int fragment, uint32_t window_length, double quality_threshold,
+                          double error_threshold, uint32_t threads, uint64_t* nbytes) {
+    PolishOptions opt;
+    opt.fragment = fragment != 0;
+    opt.window_length = window_length;
+    opt.quality_threshold = quality_threshold;
+    opt.error_threshold = error_threshold;
+    opt.threads = threads;
+    std::vector<DumpedWindow> ws;
+    if (collect_windows(sequences, overlaps, targets, opt, ws)) return nullptr;
+    std::string b;
+    auto put = [&](const void* p, size_t n) { b.append(static_cast<const char*>(p), n); };
+    const uint64_t nw = ws.size();
+    put(&nw, 8);
+    for (const auto& w : ws) {
+        const uint32_t bl = uint32_t(w.backbone.size()), nl = uint32_t(w.seqs.size());
+        const uint8_t tgs = w.tgs ? 1 : 0;
+        put(&w.target_id, 8);
+        put(&w.rank, 4);
+        put(&tgs, 1);
+        put(&bl, 4);
+        put(&nl, 4);
+        put(w.backbone.data(), bl);
+        put(w.backbone_qual.data(), bl);
+        for (uint32_t i = 0; i < nl; ++i) {
+            const uint32_t len = uint32_t(w.seqs[i].size());
+            const uint8_t hq = w.quals[i].empty() ? 0 : 1;
+            put(&len, 4);
+            put(&w.positions[i].first, 4);
+            put(&w.positions[i].second, 4);
+            put(&hq, 1);
+            put(w.seqs[i].data(), len);
+            if (hq) put(w.quals[i].data(), len);
+        }
+    }
+    char* out = static_cast<char*>(malloc(b.size()));
+    memcpy(out, b.data(), b.size());
+    *nbytes = b.size();
+    return out;
+}
+
+}  // extern "C"

@@ -1,0 +1,300 @@
+"""racon_b200: racon's polishing hot path (overlap alignment + window POA
+consensus) on the NVIDIA B200.
+
+This module is the Python mirror of the C ABI in include/racon_b200.h,
+loaded with ctypes from the in-tree library racon_b200/lib/libracon_b200.so
+(built by racon_b200/build.py). It exposes:
+
+  Context(device, match, mismatch, gap, window_length)
+      .align(pairs, want_cigar)      -> device edit distance / CIGAR / breaking
+                                        points (racon src/overlap.cpp:179-292)
+      .cigar_breakpoints(overlaps)   -> breaking points from SAM CIGARs
+      .poa(windows, trim)            -> window consensus (src/window.cpp:65-142)
+      .poa_stage / poa_run / poa_fetch, align_stage / align_run / align_fetch
+  polish_files(...)                  -> racon's whole pipeline (createPolisher +
+                                        initialize + polish, src/main.cpp:152-166)
+
+There is no CPU fallback: if the library is missing or no B200 is present,
+the calls raise.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libracon_b200.so")
+CLI_PATH = os.path.join(_HERE, "bin", "racon_b200")
+
+RB_OK = 0
+_ERRORS = {1: "RB_ERR_ARG", 2: "RB_ERR_CUDA", 3: "RB_ERR_NOMEM", 4: "RB_ERR_DEVICE", 5: "RB_ERR_NODEV"}
+
+
+class RaconB200Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s: %s" % (_ERRORS.get(code, str(code)), msg))
+        self.code = code
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("match", ctypes.c_int8), ("mismatch", ctypes.c_int8), ("gap", ctypes.c_int8),
+                ("window_length", ctypes.c_uint32)]
+
+
+class _Pair(ctypes.Structure):
+    _fields_ = [("query", ctypes.c_char_p), ("query_length", ctypes.c_uint32),
+                ("target", ctypes.c_char_p), ("target_length", ctypes.c_uint32),
+                ("q_offset", ctypes.c_uint32), ("t_begin", ctypes.c_uint32)]
+
+
+class _AlnResult(ctypes.Structure):
+    _fields_ = [("edit_distance", ctypes.POINTER(ctypes.c_int32)),
+                ("breakpoints", ctypes.POINTER(ctypes.c_uint32)),
+                ("bp_offsets", ctypes.POINTER(ctypes.c_uint64)),
+                ("cigars", ctypes.POINTER(ctypes.c_char)),
+                ("cigar_offsets", ctypes.POINTER(ctypes.c_uint64))]
+
+
+class _CigarOverlap(ctypes.Structure):
+    _fields_ = [("cigar", ctypes.c_char_p), ("cigar_length", ctypes.c_uint32),
+                ("q_offset", ctypes.c_uint32), ("t_begin", ctypes.c_uint32), ("t_end", ctypes.c_uint32)]
+
+
+class _Window(ctypes.Structure):
+    _fields_ = [("backbone", ctypes.c_char_p), ("backbone_quality", ctypes.c_char_p),
+                ("backbone_length", ctypes.c_uint32), ("n_layers", ctypes.c_uint32),
+                ("layers", ctypes.POINTER(ctypes.c_char_p)),
+                ("layer_qualities", ctypes.POINTER(ctypes.c_char_p)),
+                ("layer_lengths", ctypes.POINTER(ctypes.c_uint32)),
+                ("begins", ctypes.POINTER(ctypes.c_uint32)), ("ends", ctypes.POINTER(ctypes.c_uint32)),
+                ("tgs", ctypes.c_uint8), ("id", ctypes.c_uint64), ("rank", ctypes.c_uint32)]
+
+
+class _PoaResult(ctypes.Structure):
+    _fields_ = [("consensus", ctypes.POINTER(ctypes.c_char)), ("offsets", ctypes.POINTER(ctypes.c_uint64)),
+                ("polished", ctypes.POINTER(ctypes.c_uint8))]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("cells", ctypes.c_uint64), ("items", ctypes.c_uint64), ("max_nodes", ctypes.c_uint32),
+                ("top_kernel_ms", ctypes.c_double)]
+
+
+_lib = None
+
+
+def load():
+    """Loads the in-tree native library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RaconB200Error(5, "native library missing: %s (run racon_b200/build.py)" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    lib.rb_create.restype = vp
+    lib.rb_create.argtypes = [ctypes.c_int, ctypes.POINTER(_Params)]
+    lib.rb_create_error.restype = ctypes.c_char_p
+    lib.rb_destroy.argtypes = [vp]
+    lib.rb_last_error.restype = ctypes.c_char_p
+    lib.rb_last_error.argtypes = [vp]
+    lib.rb_align_batch.argtypes = [vp, ctypes.POINTER(_Pair), ctypes.c_size_t, ctypes.c_int,
+                                   ctypes.POINTER(_AlnResult)]
+    lib.rb_align_stage.argtypes = [vp, ctypes.POINTER(_Pair), ctypes.c_size_t, ctypes.c_int]
+    lib.rb_align_run.argtypes = [vp]
+    lib.rb_align_fetch.argtypes = [vp, ctypes.POINTER(_AlnResult)]
+    lib.rb_cigar_breakpoints.argtypes = [vp, ctypes.POINTER(_CigarOverlap), ctypes.c_size_t,
+                                         ctypes.POINTER(_AlnResult)]
+    lib.rb_poa_batch.argtypes = [vp, ctypes.POINTER(_Window), ctypes.c_size_t, ctypes.c_int,
+                                 ctypes.POINTER(_PoaResult)]
+    lib.rb_poa_stage.argtypes = [vp, ctypes.POINTER(_Window), ctypes.c_size_t, ctypes.c_int]
+    lib.rb_poa_run.argtypes = [vp]
+    lib.rb_poa_fetch.argtypes = [vp, ctypes.POINTER(_PoaResult)]
+    lib.rb_poa_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    lib.rb_align_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    lib.rb_polish_files.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                    ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_int8, ctypes.c_int8, ctypes.c_int8, ctypes.c_uint32, ctypes.c_int,
+                                    ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                    ctypes.POINTER(ctypes.c_double)]
+    lib.rb_pipeline_error.restype = ctypes.c_char_p
+    lib.rb_free.argtypes = [vp]
+    _lib = lib
+    return lib
+
+
+def _b(s):
+    if s is None:
+        return None
+    return s.encode() if isinstance(s, str) else bytes(s)
+
+
+class Context:
+    """One device context (include/racon_b200.h rb_create)."""
+
+    def __init__(self, device=0, match=3, mismatch=-5, gap=-4, window_length=500):
+        self.lib = load()
+        p = _Params(match, mismatch, gap, window_length)
+        self.ptr = self.lib.rb_create(device, ctypes.byref(p))
+        if not self.ptr:
+            raise RaconB200Error(5, self.lib.rb_create_error().decode())
+        self.window_length = window_length
+        self._keep = None
+
+    def close(self):
+        if self.ptr:
+            self.lib.rb_destroy(self.ptr)
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != RB_OK:
+            raise RaconB200Error(rc, self.lib.rb_last_error(self.ptr).decode())
+
+    # ---- overlap alignment ----
+    def _pairs(self, pairs):
+        arr = (_Pair * max(1, len(pairs)))()
+        keep = []
+        for i, p in enumerate(pairs):
+            q, t = _b(p["query"]), _b(p["target"])
+            keep += [q, t]
+            arr[i] = _Pair(q, len(q), t, len(t), p.get("q_offset", 0), p.get("t_begin", 0))
+        return arr, keep
+
+    @staticmethod
+    def _aln_out(r, n, want_cigar):
+        out = []
+        for i in range(n):
+            b, e = r.bp_offsets[i], r.bp_offsets[i + 1]
+            bp = [(r.breakpoints[k], r.breakpoints[k + 1]) for k in range(b, e, 2)]
+            cig = None
+            if want_cigar and r.cigar_offsets:
+                cb, ce = r.cigar_offsets[i], r.cigar_offsets[i + 1]
+                cig = ctypes.string_at(ctypes.addressof(r.cigars.contents) + cb, ce - cb).decode() if ce > cb else ""
+            out.append({"edit_distance": r.edit_distance[i], "breakpoints": bp, "cigar": cig})
+        return out
+
+    def align(self, pairs, want_cigar=True):
+        """pairs: list of dicts with query, target, q_offset, t_begin."""
+        arr, keep = self._pairs(pairs)
+        r = _AlnResult()
+        self._check(self.lib.rb_align_batch(self.ptr, arr, len(pairs), int(want_cigar), ctypes.byref(r)))
+        return self._aln_out(r, len(pairs), want_cigar)
+
+    def align_stage(self, pairs, want_cigar=False):
+        arr, keep = self._pairs(pairs)
+        self._check(self.lib.rb_align_stage(self.ptr, arr, len(pairs), int(want_cigar)))
+        self._staged_pairs = len(pairs)
+        self._staged_cigar = want_cigar
+
+    def align_run(self):
+        self._check(self.lib.rb_align_run(self.ptr))
+
+    def align_fetch(self):
+        r = _AlnResult()
+        self._check(self.lib.rb_align_fetch(self.ptr, ctypes.byref(r)))
+        return self._aln_out(r, self._staged_pairs, self._staged_cigar)
+
+    def cigar_breakpoints(self, overlaps):
+        """overlaps: list of dicts with cigar, q_offset, t_begin, t_end."""
+        arr = (_CigarOverlap * max(1, len(overlaps)))()
+        keep = []
+        for i, o in enumerate(overlaps):
+            c = _b(o["cigar"])
+            keep.append(c)
+            arr[i] = _CigarOverlap(c, len(c), o["q_offset"], o["t_begin"], o["t_end"])
+        r = _AlnResult()
+        self._check(self.lib.rb_cigar_breakpoints(self.ptr, arr, len(overlaps), ctypes.byref(r)))
+        return [x["breakpoints"] for x in self._aln_out(r, len(overlaps), False)]
+
+    # ---- window consensus ----
+    def _windows(self, windows):
+        arr = (_Window * max(1, len(windows)))()
+        keep = []
+        for i, w in enumerate(windows):
+            bb = _b(w["backbone"])
+            bq = _b(w.get("backbone_quality"))
+            layers = [_b(s) for s in w["layers"]]
+            quals = [_b(q) for q in w.get("qualities", [None] * len(layers))]
+            n = len(layers)
+            la = (ctypes.c_char_p * max(1, n))(*layers)
+            qa = (ctypes.c_char_p * max(1, n))(*quals)
+            ll = (ctypes.c_uint32 * max(1, n))(*[len(s) for s in layers])
+            bg = (ctypes.c_uint32 * max(1, n))(*w["begins"])
+            en = (ctypes.c_uint32 * max(1, n))(*w["ends"])
+            keep += [bb, bq, layers, quals, la, qa, ll, bg, en]
+            arr[i] = _Window(bb, bq, len(bb), n, la, qa, ll, bg, en, int(w.get("tgs", 1)), w.get("id", 0),
+                             w.get("rank", 0))
+        return arr, keep
+
+    @staticmethod
+    def _poa_out(r, n):
+        out = []
+        base = ctypes.addressof(r.consensus.contents) if n else 0
+        for i in range(n):
+            b, e = r.offsets[i], r.offsets[i + 1]
+            out.append((ctypes.string_at(base + b, e - b).decode() if e > b else "", bool(r.polished[i])))
+        return out
+
+    def poa(self, windows, trim=True):
+        """windows: list of dicts (backbone, backbone_quality, layers, qualities,
+        begins, ends, tgs). Returns [(consensus, polished)]."""
+        arr, keep = self._windows(windows)
+        r = _PoaResult()
+        self._check(self.lib.rb_poa_batch(self.ptr, arr, len(windows), int(trim), ctypes.byref(r)))
+        return self._poa_out(r, len(windows))
+
+    def poa_stage(self, windows, trim=True):
+        arr, keep = self._windows(windows)
+        self._check(self.lib.rb_poa_stage(self.ptr, arr, len(windows), int(trim)))
+        self._staged_windows = len(windows)
+
+    def poa_run(self):
+        self._check(self.lib.rb_poa_run(self.ptr))
+
+    def poa_fetch(self):
+        r = _PoaResult()
+        self._check(self.lib.rb_poa_fetch(self.ptr, ctypes.byref(r)))
+        return self._poa_out(r, self._staged_windows)
+
+    def poa_stats(self):
+        s = Stats()
+        self._check(self.lib.rb_poa_stats(self.ptr, ctypes.byref(s)))
+        return s
+
+    def align_stats(self):
+        s = Stats()
+        self._check(self.lib.rb_align_stats(self.ptr, ctypes.byref(s)))
+        return s
+
+
+def polish_files(sequences, overlaps, targets, fragment=False, window_length=500, quality_threshold=10.0,
+                 error_threshold=0.3, trim=True, match=3, mismatch=-5, gap=-4, threads=1,
+                 drop_unpolished=True, device=0, stage_seconds=None):
+    """racon's pipeline on the device; returns the polished FASTA text."""
+    lib = load()
+    out = ctypes.c_void_p()
+    st = (ctypes.c_double * 4)()
+    rc = lib.rb_polish_files(_b(sequences), _b(overlaps), _b(targets), int(fragment), window_length,
+                             quality_threshold, error_threshold, int(trim), match, mismatch, gap, threads,
+                             int(drop_unpolished), device, ctypes.byref(out), st)
+    if rc != RB_OK:
+        raise RaconB200Error(rc, lib.rb_pipeline_error().decode())
+    try:
+        text = ctypes.string_at(out.value).decode()
+    finally:
+        lib.rb_free(out)
+    if stage_seconds is not None:
+        stage_seconds[:] = list(st)
+    return text

@@ -1,0 +1,133 @@
+// racon's C++ polishing API (drop-in for the reference's src/polisher.hpp:36-98
+// and src/sequence.hpp:26-74), backed by the B200 device path.
+//
+// createPolisher keeps the reference signature (src/polisher.hpp:42-48,
+// including the CUDA-plug-in arguments, which are accepted and ignored: the
+// device path is always used). Polisher::initialize and Polisher::polish keep
+// their signatures and behaviour; the two protected virtuals that the
+// reference's CUDA plug-in overrides (find_overlap_breaking_points,
+// src/polisher.hpp:75, and polish) run on the device through the C ABI in
+// include/racon_b200.h. There is no CPU path.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+struct rb_ctx;
+
+namespace racon {
+
+class Sequence {
+public:
+    ~Sequence() = default;
+    const std::string& name() const { return name_; }
+    const std::string& data() const { return data_; }
+    const std::string& reverse_complement() const { return reverse_complement_; }
+    const std::string& quality() const { return quality_; }
+    const std::string& reverse_quality() const { return reverse_quality_; }
+    void create_reverse_complement();
+    void transmute(bool has_name, bool has_data, bool has_reverse_data);
+
+    // FASTA record (data uppercased)
+    Sequence(const char* name, uint32_t name_length, const char* data, uint32_t data_length);
+    // FASTQ record; the quality is dropped when every value is '!'
+    Sequence(const char* name, uint32_t name_length, const char* data, uint32_t data_length,
+             const char* quality, uint32_t quality_length);
+    Sequence(const std::string& name, const std::string& data);
+    Sequence(const Sequence&) = delete;
+    const Sequence& operator=(const Sequence&) = delete;
+
+private:
+    std::string name_;
+    std::string data_;
+    std::string reverse_complement_;
+    std::string quality_;
+    std::string reverse_quality_;
+};
+
+std::unique_ptr<Sequence> createSequence(const std::string& name, const std::string& data);
+
+enum class PolisherType {
+    kC,  // contig polishing
+    kF   // fragment error correction
+};
+
+class Overlap;
+class Window;
+
+class Polisher;
+std::unique_ptr<Polisher> createPolisher(const std::string& sequences_path,
+    const std::string& overlaps_path, const std::string& target_path,
+    PolisherType type, uint32_t window_length, double quality_threshold,
+    double error_threshold, bool trim, int8_t match, int8_t mismatch, int8_t gap,
+    uint32_t num_threads, uint32_t cuda_batches = 0,
+    bool cuda_banded_alignment = false, uint32_t cudaaligner_batches = 0,
+    uint32_t cudaaligner_band_width = 0);
+
+class Polisher {
+public:
+    virtual ~Polisher();
+
+    virtual void initialize();
+
+    virtual void polish(std::vector<std::unique_ptr<Sequence>>& dst,
+        bool drop_unpolished_sequences);
+
+    // CUDA device used by this polisher (default 0, or RACON_B200_DEVICE)
+    int device() const { return device_; }
+    // wall seconds of the stages of the last run: load, align, layers, consensus
+    const double* stage_seconds() const { return stage_s_; }
+
+    friend std::unique_ptr<Polisher> createPolisher(const std::string& sequences_path,
+        const std::string& overlaps_path, const std::string& target_path,
+        PolisherType type, uint32_t window_length, double quality_threshold,
+        double error_threshold, bool trim, int8_t match, int8_t mismatch, int8_t gap,
+        uint32_t num_threads, uint32_t cuda_batches, bool cuda_banded_alignment,
+        uint32_t cudaaligner_batches, uint32_t cudaaligner_band_width);
+
+protected:
+    Polisher(const std::string& sequences_path, const std::string& overlaps_path,
+        const std::string& target_path, int sequences_format, int overlaps_format,
+        int target_format, PolisherType type, uint32_t window_length,
+        double quality_threshold, double error_threshold, bool trim, int8_t match,
+        int8_t mismatch, int8_t gap, uint32_t num_threads);
+    Polisher(const Polisher&) = delete;
+    const Polisher& operator=(const Polisher&) = delete;
+    virtual void find_overlap_breaking_points(std::vector<std::unique_ptr<Overlap>>& overlaps);
+
+    std::string sequences_path_, overlaps_path_, target_path_;
+    int sequences_format_, overlaps_format_, target_format_;
+
+    PolisherType type_;
+    double quality_threshold_;
+    double error_threshold_;
+    bool trim_;
+    int8_t match_, mismatch_, gap_;
+
+    std::vector<std::unique_ptr<Sequence>> sequences_;
+    std::vector<uint32_t> targets_coverages_;
+    std::string dummy_quality_;
+
+    uint32_t window_length_;
+    std::vector<std::shared_ptr<Window>> windows_;
+    bool tgs_ = true;
+
+    uint32_t num_threads_;
+    int device_ = 0;
+    rb_ctx* ctx_ = nullptr;
+    double stage_s_[4] = {0, 0, 0, 0};
+};
+
+// Creates the polisher and runs initialize + polish; used by the CLI and the
+// C entry point rb_polish_files. Returns the polished records.
+std::vector<std::unique_ptr<Sequence>> polish_files(const std::string& sequences_path,
+    const std::string& overlaps_path, const std::string& target_path, PolisherType type,
+    uint32_t window_length, double quality_threshold, double error_threshold, bool trim,
+    int8_t match, int8_t mismatch, int8_t gap, uint32_t num_threads, bool drop_unpolished,
+    double* stage_seconds);
+
+}  // namespace racon

@@ -1,0 +1,1175 @@
+// Overlap alignment on the device: edit distance, alignment path and window
+// breaking points with the semantics of racon's
+//   src/overlap.cpp:205-224  edlibAlign(NW, PATH, k = -1) + standard CIGAR
+//   src/overlap.cpp:226-292  find_breaking_points_from_cigar
+//
+// Design (B200, sm_100a). One warp owns one subproblem at a time; warps are
+// persistent and pull work from an atomic queue (pairs sorted by size).
+//
+// * Block sweep. The query is cut into 64-row blocks (one uint64 of vertical
+//   +1/-1 delta bits per block, Myers 1999 / Hyyro). Blocks are grouped into
+//   strips of 32, one block per lane; a strip is swept as a diagonal wavefront
+//   (lane l works on column c - l), the horizontal carry of each column moves
+//   one lane down per step through a warp shuffle, and the bottom lane's carry
+//   is kept in a per-warp column buffer for the next strip.
+// * Band. Only blocks that meet the Ukkonen band of the subproblem are
+//   computed: a cell (r, c) can lie on a path of cost <= k only if
+//   |r - c| + |(m - n) - (r - c)| <= k, i.e. r - c in
+//   [ceil((m-n-k)/2), floor((m-n+k)/2)]. Cells outside the band are taken as
+//   the cost of a real (not necessarily optimal) path, so every computed value
+//   is an upper bound and every cell on an optimal path is exact. Therefore
+//   the edit distance, the Hirschberg split row and every traceback decision
+//   equal those of the unbanded dynamic program.
+// * Distance. k doubles from max(64, |m - n|) until the band holds the corner
+//   (the first k >= distance returns the exact distance).
+// * Path. edlib's recursion is followed exactly: a subproblem is traced back
+//   from stored columns when (2*8+4) * ceil(m/64) * n < 1 MiB, else it is
+//   split at target column n/2: forward sweep of the left half and reverse
+//   sweep of the right half capture one column each, the split row is the
+//   first query row whose two halves sum to the subproblem's score, then the
+//   row -1 and row m-1 boundaries. Levels of the recursion tree are processed
+//   breadth-first, one launch per level.
+// * Traceback. The leaf sweep stores, per (column, band block), the vertical
+//   +1 bits after the step and the horizontal +1 bits of the step. At a cell
+//   the walk moves up (query base inserted) if the vertical bit is set, left
+//   (target base deleted) if the horizontal bit is set, else diagonally -
+//   edlib's preference order. The 32 lanes prefetch 32 columns; the row is
+//   passed lane to lane.
+// * Output. The path is recorded as mq[t] = matched query position or -1 for
+//   every target position. An optimal alignment never has an insertion next
+//   to a deletion (a diagonal step is cheaper), so the op string, the CIGAR
+//   and racon's breaking points all follow from mq.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "rb_internal.hpp"
+
+namespace rb {
+namespace {
+
+typedef unsigned long long u64;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarpsPerBlock = 4;
+constexpr int kMaxSym = 32;
+constexpr long long kLeafBytes = 1024 * 1024;  // edlib's traceback threshold
+
+enum NwStatus : int {
+    kNwOk = 0,
+    kNwSplitMissing = 1,
+    kNwTraceOutOfBand = 2,
+    kNwTaskOverflow = 3,
+    kNwBadSymbol = 4,
+};
+
+struct NwTask {
+    uint32_t pair;
+    uint32_t qa, m;
+    uint32_t ta, n;
+    int32_t score;
+};
+
+struct NwDevArgs {
+    const uint8_t* codes;
+    const NwPairDev* pairs;
+    const uint32_t* order;
+    uint32_t npairs;
+    int32_t* dist;
+    int32_t* mq;
+    uint32_t* bp;
+    uint32_t* bp_count;
+    uint32_t window_length;
+    // per-warp scratch
+    uint8_t* scratch;
+    size_t scratch_stride;
+    uint32_t scratch_warps;
+    uint32_t max_n, max_nb;
+    // work queues
+    unsigned int* counters;  // [0] pair/task cursor, [1] next-level count, [2] status
+    const NwTask* tasks_in;
+    uint32_t ntasks_in;
+    NwTask* tasks_out;
+    uint32_t tasks_out_cap;
+};
+
+__device__ __forceinline__ int fdiv64(int a) { return a >= 0 ? a / 64 : -((-a + 63) / 64); }
+__device__ __forceinline__ int fdiv2(int a) { return a >= 0 ? a / 2 : -((-a + 1) / 2); }
+
+struct Band {
+    int m, n, k, dlo, dhi, nb;
+};
+
+__device__ __forceinline__ Band make_band(int m, int n, int k) {
+    Band B;
+    B.m = m;
+    B.n = n;
+    B.k = k;
+    const int d = m - n;
+    B.dlo = -fdiv2(k - d);  // ceil((d - k) / 2)
+    B.dhi = fdiv2(d + k);   // floor((d + k) / 2)
+    B.nb = (m + 63) / 64;
+    return B;
+}
+__device__ __forceinline__ int band_lo_block(const Band& B, int c) { return max(0, fdiv64(c + B.dlo)); }
+__device__ __forceinline__ int band_hi_block(const Band& B, int c) {
+    return min(B.nb - 1, fdiv64(c + B.dhi));
+}
+
+__device__ __forceinline__ int myers_step(u64& pv, u64& mv, u64 eq, int hin, u64& ph_out) {
+    const u64 neg = hin < 0 ? 1ull : 0ull;
+    const u64 xv = eq | mv;
+    eq |= neg;
+    const u64 xh = (((eq & pv) + pv) ^ pv) | eq;
+    u64 ph = mv | ~(xh | pv);
+    u64 mh = pv & xh;
+    ph_out = ph;
+    const int hout = int(ph >> 63) - int(mh >> 63);
+    ph = (ph << 1) | (hin > 0 ? 1ull : 0ull);
+    mh = (mh << 1) | neg;
+    pv = mh | ~(xv | ph);
+    mv = ph & xv;
+    return hout;
+}
+
+// Value of row i (0..63) of a block whose last row holds `score`.
+__device__ __forceinline__ int block_value(u64 pv, u64 mv, int score, int i) {
+    if (i == 63) return score;
+    return score - __popcll(pv >> (i + 1)) + __popcll(mv >> (i + 1));
+}
+
+__device__ __forceinline__ void set_status(unsigned int* counters, int code) {
+    atomicCAS(&counters[2], 0u, unsigned(code));
+}
+
+// Per-warp scratch layout.
+struct WarpScratch {
+    int8_t* carry_h[2];
+    int32_t* carry_s[2];
+    u64* capl_pv;
+    u64* capl_mv;
+    int32_t* capl_sc;
+    u64* capr_pv;
+    u64* capr_mv;
+    int32_t* capr_sc;
+    uint4* leaf;
+};
+
+__device__ WarpScratch warp_scratch(const NwDevArgs& a, uint32_t slot) {
+    uint8_t* p = a.scratch + size_t(slot) * a.scratch_stride;
+    WarpScratch w;
+    const size_t n = a.max_n, nb = a.max_nb;
+    auto take = [&](size_t bytes) {
+        uint8_t* r = p;
+        p += (bytes + 255) & ~size_t(255);
+        return r;
+    };
+    w.carry_h[0] = reinterpret_cast<int8_t*>(take(n));
+    w.carry_h[1] = reinterpret_cast<int8_t*>(take(n));
+    w.carry_s[0] = reinterpret_cast<int32_t*>(take(n * 4));
+    w.carry_s[1] = reinterpret_cast<int32_t*>(take(n * 4));
+    w.capl_pv = reinterpret_cast<u64*>(take(nb * 8));
+    w.capl_mv = reinterpret_cast<u64*>(take(nb * 8));
+    w.capl_sc = reinterpret_cast<int32_t*>(take(nb * 4));
+    w.capr_pv = reinterpret_cast<u64*>(take(nb * 8));
+    w.capr_mv = reinterpret_cast<u64*>(take(nb * 8));
+    w.capr_sc = reinterpret_cast<int32_t*>(take(nb * 4));
+    w.leaf = reinterpret_cast<uint4*>(take(kLeafBytes));
+    return w;
+}
+
+size_t warp_scratch_bytes(size_t n, size_t nb) {
+    auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
+    return 2 * r(n) + 2 * r(n * 4) + 2 * (2 * r(nb * 8) + r(nb * 4)) + r(kLeafBytes);
+}
+
+enum SweepMode { kDistance = 0, kCapture = 1, kLeaf = 2 };
+
+struct SweepIO {
+    const uint8_t* q;  // subproblem query codes (forward start)
+    const uint8_t* t;  // subproblem target codes (forward start)
+    bool rev;          // sweep the reversed subproblem
+    int ncols;         // columns swept: [0, ncols)
+    int nsym;
+    u64* peq;          // shared memory, [kMaxSym][32] per warp
+    u64* cap_pv;
+    u64* cap_mv;
+    int32_t* cap_sc;
+    uint4* leaf;
+    int bw;            // leaf: blocks stored per column
+};
+
+// Banded block sweep of one subproblem by one warp. MODE kDistance returns
+// the value of cell (m-1, n-1) (INT_MAX if the band never reached it).
+template <int MODE>
+__device__ int warp_sweep(const SweepIO& io, const Band& B, const WarpScratch& ws, int lane,
+                          unsigned int* counters) {
+    int result = INT_MAX;
+    const int nstrips = (B.nb + 31) / 32;
+    const int m = B.m, n = B.n;
+    for (int s = 0; s < nstrips; ++s) {
+        const int b = 32 * s + lane;
+        const bool lane_valid = b < B.nb;
+        const int cb_lo = max(0, 64 * b - B.dhi);
+        const int cb_hi = min(io.ncols - 1, 64 * b + 63 - B.dlo);
+        const int s_lo = max(0, 64 * 32 * s - B.dhi);
+        const int last_b = min(B.nb - 1, 32 * s + 31);
+        const int s_hi = min(io.ncols - 1, 64 * last_b + 63 - B.dlo);
+        if (s_lo > s_hi) break;  // the band leaves the swept columns above this strip
+        const int prev_hi = min(io.ncols - 1, 64 * 32 * s - 1 - B.dlo);
+
+        // query bit masks of this lane's block
+        for (int sym = 0; sym < io.nsym; ++sym) io.peq[sym * 32 + lane] = 0ull;
+        if (lane_valid) {
+            const int r0 = 64 * b;
+            const int rows = min(64, m - r0);
+            for (int i = 0; i < rows; ++i) {
+                const int r = r0 + i;
+                const int code = io.rev ? io.q[m - 1 - r] : io.q[r];
+                io.peq[code * 32 + lane] |= (1ull << i);
+            }
+            if (rows < 64) {
+                const u64 pad = ~0ull << rows;  // rows past the query end match anything
+                for (int sym = 0; sym < io.nsym; ++sym) io.peq[sym * 32 + lane] |= pad;
+            }
+        }
+        __syncwarp();
+
+        u64 pv = 0, mv = 0;
+        int score = 0;
+        bool started = false;
+        int in_pack = 0;  // previous step of lane-1: (score << 3) | (processed << 2) | (hout + 1)
+        const int steps = (s_hi - s_lo) + 32;
+        int8_t* carry_h_out = ws.carry_h[s & 1];
+        int32_t* carry_s_out = ws.carry_s[s & 1];
+        const int8_t* carry_h_in = ws.carry_h[(s + 1) & 1];
+        const int32_t* carry_s_in = ws.carry_s[(s + 1) & 1];
+        for (int st = 0; st < steps; ++st) {
+            const int c = s_lo + st - lane;
+            const bool active = lane_valid && c >= cb_lo && c <= cb_hi;
+            int hout = 0;
+            if (active) {
+                const int up_h = (in_pack & 3) - 1;
+                const bool up_proc = (in_pack >> 2) & 1;
+                const int up_score = in_pack >> 3;
+                int hin;
+                if (lane == 0) {
+                    hin = (s == 0 || c > prev_hi) ? 1 : int(carry_h_in[c]);
+                } else {
+                    hin = up_proc ? up_h : 1;
+                }
+                if (!started) {
+                    started = true;
+                    pv = ~0ull;
+                    mv = 0ull;
+                    if (c == 0) {
+                        score = 64 * (b + 1);
+                    } else {
+                        const int v = (lane == 0) ? carry_s_in[c - 1]
+                                                  : (up_proc ? up_score - up_h : up_score);
+                        score = v + 64;
+                    }
+                }
+                const int tc = io.rev ? io.t[n - 1 - c] : io.t[c];
+                const u64 eq = io.peq[tc * 32 + lane];
+                u64 ph;
+                hout = myers_step(pv, mv, eq, hin, ph);
+                score += hout;
+                if (MODE == kLeaf) {
+                    const int blo = band_lo_block(B, c);
+                    io.leaf[size_t(c) * io.bw + (b - blo)] =
+                        make_uint4(unsigned(pv), unsigned(pv >> 32), unsigned(ph), unsigned(ph >> 32));
+                }
+                if (MODE == kCapture && c == io.ncols - 1) {
+                    io.cap_pv[b] = pv;
+                    io.cap_mv[b] = mv;
+                    io.cap_sc[b] = score;
+                }
+                if (MODE == kDistance && b == B.nb - 1 && c == n - 1) {
+                    result = block_value(pv, mv, score, (m - 1) & 63);
+                }
+                if (lane == 31) {
+                    carry_h_out[c] = int8_t(hout);
+                    carry_s_out[c] = score;
+                }
+            }
+            const int pack = (score << 3) | ((active ? 1 : 0) << 2) | (hout + 1);
+            in_pack = __shfl_up_sync(kFull, pack, 1);
+        }
+        __syncwarp();
+    }
+    if (MODE == kDistance) {
+        for (int o = 16; o > 0; o >>= 1) result = min(result, __shfl_xor_sync(kFull, result, o));
+    }
+    (void)counters;
+    return result;
+}
+
+__device__ void fill_deleted(int32_t* mq, int from, int count, int lane) {
+    for (int i = lane; i < count; i += 32) mq[from + i] = -1;
+}
+
+// Leaf: store the band of every column, then walk back from (m-1, n-1).
+__device__ void leaf_traceback(const NwDevArgs& a, const NwPairDev& P, const NwTask& T,
+                               const WarpScratch& ws, u64* peq, int lane) {
+    const int m = int(T.m), n = int(T.n);
+    int32_t* mq = a.mq + P.mq_off + T.ta;
+    const Band B = make_band(m, n, T.score);
+    const int bw = min(B.nb, (B.dhi - B.dlo) / 64 + 2);
+    SweepIO io;
+    io.q = a.codes + P.q_off + T.qa;
+    io.t = a.codes + P.t_off + T.ta;
+    io.rev = false;
+    io.ncols = n;
+    io.nsym = int(P.nsym);
+    io.peq = peq;
+    io.leaf = ws.leaf;
+    io.bw = bw;
+    warp_sweep<kLeaf>(io, B, ws, lane, a.counters);
+    __syncwarp();
+
+    int row = m - 1;
+    int c0 = n - 1;
+    while (c0 >= 0) {
+        const int c = c0 - lane;
+        const bool has = c >= 0;
+        // prefetch the blocks holding the entry row and the one above it
+        u64 pva = 0, pha = 0, pvb = 0, phb = 0;
+        const int ba = row >= 0 ? row / 64 : -1;
+        int clo = 0, chi = -1;
+        if (has) {
+            clo = band_lo_block(B, c);
+            chi = band_hi_block(B, c);
+            if (ba >= clo && ba <= chi) {
+                const uint4 e = ws.leaf[size_t(c) * bw + (ba - clo)];
+                pva = (u64(e.y) << 32) | e.x;
+                pha = (u64(e.w) << 32) | e.z;
+            }
+            if (ba - 1 >= clo && ba - 1 <= chi) {
+                const uint4 e = ws.leaf[size_t(c) * bw + (ba - 1 - clo)];
+                pvb = (u64(e.y) << 32) | e.x;
+                phb = (u64(e.w) << 32) | e.z;
+            }
+        }
+        int r = row;
+        int my_mq = -1;
+        int r_out = r;
+        for (int l = 0; l < 32; ++l) {
+            if (c0 - l < 0) break;
+            if (lane == l) {
+                if (r < 0) {
+                    my_mq = -1;
+                    r_out = -1;
+                } else {
+                    int rr = r;
+                    bool found = false;
+                    while (rr >= 0) {
+                        const int bb = rr >> 6, i = rr & 63;
+                        u64 pvw, phw;
+                        if (bb == ba) {
+                            pvw = pva;
+                            phw = pha;
+                        } else if (bb == ba - 1) {
+                            pvw = pvb;
+                            phw = phb;
+                        } else if (bb >= clo && bb <= chi) {
+                            const uint4 e = ws.leaf[size_t(c) * bw + (bb - clo)];
+                            pvw = (u64(e.y) << 32) | e.x;
+                            phw = (u64(e.w) << 32) | e.z;
+                        } else {
+                            set_status(a.counters, kNwTraceOutOfBand);
+                            break;
+                        }
+                        if (bb < clo || bb > chi) {
+                            set_status(a.counters, kNwTraceOutOfBand);
+                            break;
+                        }
+                        const u64 lowmask = (i == 63) ? ~0ull : ((2ull << i) - 1ull);
+                        const u64 clear = ~pvw & lowmask;
+                        if (clear) {
+                            const int ip = 63 - __clzll(clear);
+                            rr = 64 * bb + ip;
+                            found = true;
+                            if ((phw >> ip) & 1ull) {
+                                my_mq = -1;
+                                r_out = rr;
+                            } else {
+                                my_mq = rr;
+                                r_out = rr - 1;
+                            }
+                            break;
+                        }
+                        rr = 64 * bb - 1;
+                    }
+                    if (!found) {
+                        my_mq = -1;
+                        r_out = -1;
+                    }
+                }
+            }
+            r = __shfl_sync(kFull, r_out, l);
+        }
+        if (has) mq[c] = my_mq >= 0 ? int(T.qa) + my_mq : -1;
+        row = r;
+        c0 -= 32;
+    }
+}
+
+__device__ void hirschberg_split(const NwDevArgs& a, const NwPairDev& P, const NwTask& T,
+                                 const WarpScratch& ws, u64* peq, int lane) {
+    const int m = int(T.m), n = int(T.n);
+    const int best = T.score;
+    const int lw = n / 2, rw = n - lw;
+    const Band B = make_band(m, n, best);
+    SweepIO io;
+    io.q = a.codes + P.q_off + T.qa;
+    io.t = a.codes + P.t_off + T.ta;
+    io.nsym = int(P.nsym);
+    io.peq = peq;
+    io.leaf = nullptr;
+    io.bw = 0;
+    io.rev = false;
+    io.ncols = lw;
+    io.cap_pv = ws.capl_pv;
+    io.cap_mv = ws.capl_mv;
+    io.cap_sc = ws.capl_sc;
+    warp_sweep<kCapture>(io, B, ws, lane, a.counters);
+    io.rev = true;
+    io.ncols = rw;
+    io.cap_pv = ws.capr_pv;
+    io.cap_mv = ws.capr_mv;
+    io.cap_sc = ws.capr_sc;
+    warp_sweep<kCapture>(io, B, ws, lane, a.counters);
+    __syncwarp();
+
+    const int llo = band_lo_block(B, lw - 1), lhi = band_hi_block(B, lw - 1);
+    const int rlo = band_lo_block(B, rw - 1), rhi = band_hi_block(B, rw - 1);
+    auto left = [&](int r) -> int {  // D(q[0..r], t[0..lw-1])
+        const int bb = r >> 6;
+        if (bb < llo || bb > lhi) return INT_MAX / 4;
+        return block_value(ws.capl_pv[bb], ws.capl_mv[bb], ws.capl_sc[bb], r & 63);
+    };
+    auto right = [&](int r) -> int {  // D(q[r..m-1], t[lw..n-1])
+        const int rr = m - 1 - r;
+        const int bb = rr >> 6;
+        if (bb < rlo || bb > rhi) return INT_MAX / 4;
+        return block_value(ws.capr_pv[bb], ws.capr_mv[bb], ws.capr_sc[bb], rr & 63);
+    };
+    const int q_lo = max(max(0, 64 * llo), m - 2 - min(m - 1, 64 * rhi + 63));
+    const int q_hi = min(min(m - 2, min(m - 1, 64 * lhi + 63)), m - 2 - 64 * rlo);
+    int split = -2, ls = 0, rs = 0;
+    for (int base = q_lo; base <= q_hi; base += 32) {
+        const int qi = base + lane;
+        int lv = 0, rv = 0;
+        bool ok = false;
+        if (qi <= q_hi) {
+            lv = left(qi);
+            rv = right(qi + 1);
+            ok = lv + rv == best;
+        }
+        const unsigned hit = __ballot_sync(kFull, ok);
+        if (hit) {
+            const int src = __ffs(hit) - 1;
+            split = base + src;
+            ls = __shfl_sync(kFull, lv, src);
+            rs = __shfl_sync(kFull, rv, src);
+            break;
+        }
+    }
+    if (split == -2) {
+        const int rv = right(0);
+        if (lw + rv == best) {
+            split = -1;
+            ls = lw;
+            rs = rv;
+        }
+    }
+    if (split == -2) {
+        const int lv = left(m - 1);
+        if (lv + rw == best) {
+            split = m - 1;
+            ls = lv;
+            rs = rw;
+        }
+    }
+    if (split == -2) {
+        if (lane == 0) set_status(a.counters, kNwSplitMissing);
+        return;
+    }
+    const int uh = split + 1;
+    int32_t* mq = a.mq + P.mq_off;
+    NwTask kids[2];
+    kids[0] = NwTask{T.pair, T.qa, uint32_t(uh), T.ta, uint32_t(lw), ls};
+    kids[1] = NwTask{T.pair, T.qa + uh, uint32_t(m - uh), T.ta + lw, uint32_t(rw), rs};
+    for (int k = 0; k < 2; ++k) {
+        const NwTask& K = kids[k];
+        if (K.n == 0) continue;
+        if (K.m == 0) {
+            fill_deleted(mq, int(K.ta), int(K.n), lane);
+            continue;
+        }
+        if (lane == 0) {
+            const unsigned idx = atomicAdd(&a.counters[1], 1u);
+            if (idx < a.tasks_out_cap) {
+                a.tasks_out[idx] = K;
+            } else {
+                set_status(a.counters, kNwTaskOverflow);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ bool is_leaf(uint32_t m, uint32_t n) {
+    const long long nb = (m + 63) / 64;
+    return (2LL * 8 + 4) * nb * n < kLeafBytes;
+}
+
+extern __shared__ u64 g_peq_smem[];
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+nw_distance_kernel(NwDevArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t slot = blockIdx.x * kWarpsPerBlock + wib;
+    u64* peq = g_peq_smem + wib * kMaxSym * 32;
+    const WarpScratch ws = warp_scratch(a, slot);
+    while (true) {
+        unsigned i = 0;
+        if (lane == 0) i = atomicAdd(&a.counters[0], 1u);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= a.npairs) break;
+        const uint32_t pi = a.order[i];
+        const NwPairDev P = a.pairs[pi];
+        const int m = int(P.m), n = int(P.n);
+        if (m == 0 || n == 0) {
+            if (lane == 0) a.dist[pi] = max(m, n);
+            continue;
+        }
+        SweepIO io;
+        io.q = a.codes + P.q_off;
+        io.t = a.codes + P.t_off;
+        io.rev = false;
+        io.ncols = n;
+        io.nsym = int(P.nsym);
+        io.peq = peq;
+        io.leaf = nullptr;
+        io.bw = 0;
+        int k = max(64, abs(m - n));
+        int d = INT_MAX;
+        while (true) {
+            const Band B = make_band(m, n, k);
+            d = warp_sweep<kDistance>(io, B, ws, lane, a.counters);
+            if (d <= k) break;
+            k *= 2;
+        }
+        if (lane == 0) a.dist[pi] = d;
+    }
+}
+
+__global__ void nw_root_tasks_kernel(NwDevArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.npairs) return;
+    const NwPairDev P = a.pairs[i];
+    if (P.m == 0 || P.n == 0) return;  // edlib returns no alignment for an empty side
+    const unsigned idx = atomicAdd(&a.counters[1], 1u);
+    if (idx < a.tasks_out_cap) {
+        a.tasks_out[idx] = NwTask{i, 0, P.m, 0, P.n, a.dist[i]};
+    } else {
+        set_status(a.counters, kNwTaskOverflow);
+    }
+}
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+nw_level_kernel(NwDevArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t slot = blockIdx.x * kWarpsPerBlock + wib;
+    u64* peq = g_peq_smem + wib * kMaxSym * 32;
+    const WarpScratch ws = warp_scratch(a, slot);
+    while (true) {
+        unsigned i = 0;
+        if (lane == 0) i = atomicAdd(&a.counters[0], 1u);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= a.ntasks_in) break;
+        const NwTask T = a.tasks_in[i];
+        const NwPairDev P = a.pairs[T.pair];
+        if (is_leaf(T.m, T.n)) {
+            leaf_traceback(a, P, T, ws, peq, lane);
+        } else {
+            hirschberg_split(a, P, T, ws, peq, lane);
+        }
+        __syncwarp();
+    }
+}
+
+// Breaking points from mq: one window segment per floor(t / w); for each
+// segment with a match, (first match t, q) and (last match t + 1, q + 1).
+__global__ void nw_breakpoints_kernel(NwDevArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.npairs) return;
+    const NwPairDev P = a.pairs[i];
+    uint32_t* out = a.bp + P.bp_off;
+    uint32_t cnt = 0;
+    if (P.m != 0 && P.n != 0) {
+        const int32_t* mq = a.mq + P.mq_off;
+        const uint32_t w = a.window_length;
+        int64_t cur = -1;
+        uint32_t ft = 0, fq = 0, lt = 0, lq = 0;
+        for (uint32_t c = 0; c < P.n; ++c) {
+            const int32_t v = mq[c];
+            if (v < 0) continue;
+            const uint32_t t = P.t_begin + c;
+            const int64_t sgm = t / w;
+            if (sgm != cur) {
+                if (cur >= 0) {
+                    out[cnt++] = ft;
+                    out[cnt++] = fq;
+                    out[cnt++] = lt;
+                    out[cnt++] = lq;
+                }
+                cur = sgm;
+                ft = t;
+                fq = P.q_offset + uint32_t(v);
+            }
+            lt = t + 1;
+            lq = P.q_offset + uint32_t(v) + 1;
+        }
+        if (cur >= 0) {
+            out[cnt++] = ft;
+            out[cnt++] = fq;
+            out[cnt++] = lt;
+            out[cnt++] = lq;
+        }
+    }
+    a.bp_count[i] = cnt;
+}
+
+// CIGAR from mq (standard M/I/D). pass 0 counts characters, pass 1 writes.
+__device__ int put_run(char* dst, int pos, bool write, int len, char op) {
+    char tmp[12];
+    int d = 0;
+    while (len > 0) {
+        tmp[d++] = char('0' + len % 10);
+        len /= 10;
+    }
+    if (write)
+        for (int k = 0; k < d; ++k) dst[pos + k] = tmp[d - 1 - k];
+    pos += d;
+    if (write) dst[pos] = op;
+    return pos + 1;
+}
+
+__global__ void nw_cigar_kernel(NwDevArgs a, uint64_t* lens, const uint64_t* offs, char* out,
+                                int write) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.npairs) return;
+    const NwPairDev P = a.pairs[i];
+    if (P.m == 0 || P.n == 0) {
+        if (!write) lens[i] = 0;
+        return;
+    }
+    const int32_t* mq = a.mq + P.mq_off;
+    char* dst = write ? out + offs[i] : nullptr;
+    int pos = 0;
+    char run_op = 0;
+    int run_len = 0;
+    auto emit = [&](char op, int len) {
+        if (op == run_op) {
+            run_len += len;
+        } else {
+            if (run_len > 0) pos = put_run(dst, pos, write != 0, run_len, run_op);
+            run_op = op;
+            run_len = len;
+        }
+    };
+    int qprev = -1;
+    for (uint32_t c = 0; c < P.n; ++c) {
+        const int v = mq[c];
+        if (v >= 0) {
+            const int ins = v - qprev - 1;
+            if (ins > 0) emit('I', ins);
+            emit('M', 1);
+            qprev = v;
+        } else {
+            emit('D', 1);
+        }
+    }
+    const int tail = int(P.m) - 1 - qprev;
+    if (tail > 0) emit('I', tail);
+    if (run_len > 0) pos = put_run(dst, pos, write != 0, run_len, run_op);
+    if (!write) lens[i] = uint64_t(pos);
+}
+
+__global__ void exclusive_scan_kernel(const uint64_t* in, uint64_t* out, uint32_t n) {
+    // single block; n up to a few million
+    __shared__ uint64_t part[1024];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t b = tid * per, e = min(n, b + per);
+    uint64_t s = 0;
+    for (uint32_t i = b; i < e; ++i) s += in[i];
+    part[tid] = s;
+    __syncthreads();
+    if (tid == 0) {
+        uint64_t acc = 0;
+        for (uint32_t k = 0; k < blockDim.x; ++k) {
+            const uint64_t v = part[k];
+            part[k] = acc;
+            acc += v;
+        }
+        out[n] = acc;
+    }
+    __syncthreads();
+    uint64_t acc = part[tid];
+    for (uint32_t i = b; i < e; ++i) {
+        out[i] = acc;
+        acc += in[i];
+    }
+}
+
+
+// Breaking points walked from a SAM CIGAR, one thread per overlap, following
+// src/overlap.cpp:226-292 step by step (window ends at every multiple of w
+// inside (t_begin, t_end), plus t_end - 1).
+struct CigarOvlDev {
+    uint64_t cigar_off;
+    uint64_t bp_off;
+    uint32_t cigar_len, q_offset, t_begin, t_end;
+};
+
+__global__ void cigar_breakpoints_kernel(const char* cig, const CigarOvlDev* ov, uint32_t n,
+                                         uint32_t w, uint32_t* bp, uint32_t* bp_count,
+                                         unsigned int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const CigarOvlDev o = ov[i];
+    const char* c = cig + o.cigar_off;
+    uint32_t* out = bp + o.bp_off;
+    uint32_t cnt = 0;
+    // window ends in order: first multiple of w above t_begin, minus one ...
+    const uint32_t first_mult = (o.t_begin / w + 1) * w;
+    const uint32_t nmult = first_mult < o.t_end ? (o.t_end - 1 - first_mult) / w + 1 : 0;
+    uint32_t wi = 0;
+    auto window_end = [&](uint32_t k) -> int64_t {
+        return k < nmult ? int64_t(first_mult) + int64_t(k) * w - 1 : int64_t(o.t_end) - 1;
+    };
+    const uint32_t nends = nmult + 1;
+    bool found = false;
+    uint32_t ft = 0, fq = 0, lt = 0, lq = 0;
+    int64_t q_ptr = int64_t(o.q_offset) - 1;
+    int64_t t_ptr = int64_t(o.t_begin) - 1;
+    uint32_t num = 0;
+    for (uint32_t k = 0; k < o.cigar_len; ++k) {
+        const char ch = c[k];
+        if (ch >= '0' && ch <= '9') {
+            num = num * 10 + uint32_t(ch - '0');
+            continue;
+        }
+        if (ch == 'M' || ch == '=' || ch == 'X') {
+            for (uint32_t r = 0; r < num; ++r) {
+                ++q_ptr;
+                ++t_ptr;
+                if (!found) {
+                    found = true;
+                    ft = uint32_t(t_ptr);
+                    fq = uint32_t(q_ptr);
+                }
+                lt = uint32_t(t_ptr + 1);
+                lq = uint32_t(q_ptr + 1);
+                if (wi < nends && t_ptr == window_end(wi)) {
+                    out[cnt++] = ft;
+                    out[cnt++] = fq;
+                    out[cnt++] = lt;
+                    out[cnt++] = lq;
+                    found = false;
+                    ++wi;
+                }
+            }
+        } else if (ch == 'I') {
+            q_ptr += num;
+        } else if (ch == 'D' || ch == 'N') {
+            for (uint32_t r = 0; r < num; ++r) {
+                ++t_ptr;
+                if (wi < nends && t_ptr == window_end(wi)) {
+                    if (found) {
+                        out[cnt++] = ft;
+                        out[cnt++] = fq;
+                        out[cnt++] = lt;
+                        out[cnt++] = lq;
+                    }
+                    found = false;
+                    ++wi;
+                }
+            }
+        }
+        num = 0;  // S, H, P and the ops above all restart the number
+        if (t_ptr >= int64_t(o.t_end)) {
+            atomicCAS(status, 0u, 5u);
+            break;
+        }
+    }
+    bp_count[i] = cnt;
+}
+
+}  // namespace
+
+NwEngine::NwEngine(const DeviceInfo& dev, cudaStream_t stream) : dev_(dev), stream_(stream) {
+    check_cuda(cudaEventCreate(&ev0_), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&ev1_), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&ev2_), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&ev3_), "cudaEventCreate");
+    check_cuda(cudaFuncSetAttribute(nw_distance_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kWarpsPerBlock * kMaxSym * 32 * 8),
+               "cudaFuncSetAttribute");
+    check_cuda(cudaFuncSetAttribute(nw_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kWarpsPerBlock * kMaxSym * 32 * 8),
+               "cudaFuncSetAttribute");
+}
+
+NwEngine::~NwEngine() {
+    cudaEventDestroy(ev0_);
+    cudaEventDestroy(ev1_);
+    cudaEventDestroy(ev2_);
+    cudaEventDestroy(ev3_);
+}
+
+void NwEngine::stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t window_length) {
+    if (n > 0 && !pairs) throw Error{RB_ERR_ARG, "rb_align: pairs is NULL"};
+    if (window_length == 0) throw Error{RB_ERR_ARG, "rb_align: window length is 0"};
+    npairs_ = n;
+    want_cigar_ = want_cigar;
+    window_length_ = window_length;
+    // pack: per-pair symbol numbering by first appearance, query then target
+    uint64_t bytes = 0, mq_len = 0, bp_slots = 0;
+    max_m_ = max_n_ = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const rb_pair& p = pairs[i];
+        if (p.query_length > (1u << 24) || p.target_length > (1u << 24))
+            throw Error{RB_ERR_ARG, "rb_align: span longer than 2^24 bases"};
+        if ((p.query_length && !p.query) || (p.target_length && !p.target))
+            throw Error{RB_ERR_ARG, "rb_align: NULL sequence with nonzero length"};
+        bytes += ((p.query_length + 15) & ~15u) + ((p.target_length + 15) & ~15u);
+        mq_len += p.target_length;
+        if (p.target_length > 0) {
+            const uint64_t segs = (uint64_t(p.t_begin) + p.target_length - 1) / window_length -
+                                  p.t_begin / window_length + 1;
+            bp_slots += 4 * segs;
+        }
+        max_m_ = std::max(max_m_, p.query_length);
+        max_n_ = std::max(max_n_, p.target_length);
+    }
+    code_bytes_ = bytes;
+    mq_len_ = mq_len;
+    bp_slots_ = bp_slots;
+    h_codes_.reserve(std::max<uint64_t>(bytes, 16));
+    h_pairs_.reserve(std::max<size_t>(n, 1) * sizeof(NwPairDev));
+    h_order_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
+    uint8_t* codes = h_codes_.as<uint8_t>();
+    NwPairDev* pd = h_pairs_.as<NwPairDev>();
+    uint64_t off = 0, mqo = 0, bpo = 0;
+    int16_t map[256];
+    for (size_t i = 0; i < n; ++i) {
+        const rb_pair& p = pairs[i];
+        std::fill(map, map + 256, int16_t(-1));
+        int nsym = 0;
+        NwPairDev& d = pd[i];
+        d.q_off = off;
+        for (uint32_t k = 0; k < p.query_length; ++k) {
+            const uint8_t ch = uint8_t(p.query[k]);
+            if (map[ch] < 0) map[ch] = int16_t(nsym++);
+            codes[off + k] = uint8_t(map[ch]);
+        }
+        off += (p.query_length + 15) & ~15u;
+        d.t_off = off;
+        for (uint32_t k = 0; k < p.target_length; ++k) {
+            const uint8_t ch = uint8_t(p.target[k]);
+            if (map[ch] < 0) map[ch] = int16_t(nsym++);
+            codes[off + k] = uint8_t(map[ch]);
+        }
+        off += (p.target_length + 15) & ~15u;
+        if (nsym > kMaxSym) throw Error{RB_ERR_ARG, "rb_align: more than 32 distinct symbols in a pair"};
+        d.nsym = uint32_t(std::max(nsym, 1));
+        d.m = p.query_length;
+        d.n = p.target_length;
+        d.mq_off = mqo;
+        mqo += p.target_length;
+        d.bp_off = bpo;
+        if (p.target_length > 0) {
+            const uint64_t segs = (uint64_t(p.t_begin) + p.target_length - 1) / window_length -
+                                  p.t_begin / window_length + 1;
+            bpo += 4 * segs;
+        }
+        d.q_offset = p.q_offset;
+        d.t_begin = p.t_begin;
+    }
+    // size-sorted work order: largest banded work first
+    uint32_t* order = h_order_.as<uint32_t>();
+    std::iota(order, order + n, 0u);
+    std::sort(order, order + n, [&](uint32_t x, uint32_t y) {
+        const uint64_t wx = uint64_t(pd[x].m + 64) * pd[x].n, wy = uint64_t(pd[y].m + 64) * pd[y].n;
+        return wx != wy ? wx > wy : x < y;
+    });
+    d_codes_.reserve(std::max<uint64_t>(bytes, 16));
+    d_pairs_.reserve(std::max<size_t>(n, 1) * sizeof(NwPairDev));
+    d_order_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
+    d_dist_.reserve(std::max<size_t>(n, 1) * sizeof(int32_t));
+    d_mq_.reserve(std::max<uint64_t>(mq_len, 1) * sizeof(int32_t));
+    d_bp_.reserve(std::max<uint64_t>(bp_slots, 1) * sizeof(uint32_t));
+    d_bpcnt_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
+    d_misc_.reserve(64);
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    check_cuda(cudaMemcpyAsync(d_codes_.ptr, codes, bytes, cudaMemcpyHostToDevice, stream_), "H2D codes");
+    check_cuda(cudaMemcpyAsync(d_pairs_.ptr, pd, n * sizeof(NwPairDev), cudaMemcpyHostToDevice, stream_),
+               "H2D pairs");
+    check_cuda(cudaMemcpyAsync(d_order_.ptr, order, n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_),
+               "H2D order");
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    check_cuda(cudaStreamSynchronize(stream_), "stage sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.h2d_ms = ms;
+    stats_.h2d_bytes = bytes + n * (sizeof(NwPairDev) + sizeof(uint32_t));
+}
+
+void NwEngine::reserve_scratch(uint32_t max_m, uint32_t max_n) {
+    const size_t nb = (size_t(max_m) + 63) / 64 + 1;
+    const size_t ncols = size_t(max_n) + 64;
+    scratch_stride_ = warp_scratch_bytes(ncols, nb);
+    // warps: enough to fill the GPU, bounded by a scratch budget of 4 GiB
+    size_t warps = size_t(dev_.sm_count) * 16;
+    const size_t budget = size_t(4) << 30;
+    while (warps > size_t(kWarpsPerBlock) && warps * scratch_stride_ > budget) warps /= 2;
+    warps = (warps / kWarpsPerBlock) * kWarpsPerBlock;
+    if (warps == 0) warps = kWarpsPerBlock;
+    scratch_warps_ = warps;
+    d_scratch_.reserve(warps * scratch_stride_);
+}
+
+void NwEngine::run() {
+    const size_t n = npairs_;
+    stats_.launches = 0;
+    stats_.items = n;
+    stats_.cells = 0;
+    if (n == 0) {
+        stats_.kernel_ms = 0;
+        return;
+    }
+    reserve_scratch(max_m_, max_n_);
+    size_t task_cap = std::max<size_t>(n, 1) * 2 + 64;
+    d_tasks_[0].reserve(task_cap * sizeof(NwTask));
+    d_tasks_[1].reserve(task_cap * sizeof(NwTask));
+    NwDevArgs a;
+    memset(&a, 0, sizeof(a));
+    a.codes = d_codes_.as<uint8_t>();
+    a.pairs = d_pairs_.as<NwPairDev>();
+    a.order = d_order_.as<uint32_t>();
+    a.npairs = uint32_t(n);
+    a.dist = d_dist_.as<int32_t>();
+    a.mq = d_mq_.as<int32_t>();
+    a.bp = d_bp_.as<uint32_t>();
+    a.bp_count = d_bpcnt_.as<uint32_t>();
+    a.window_length = window_length_;
+    a.scratch = d_scratch_.as<uint8_t>();
+    a.scratch_stride = scratch_stride_;
+    a.scratch_warps = uint32_t(scratch_warps_);
+    a.max_n = max_n_ + 64;
+    a.max_nb = (max_m_ + 63) / 64 + 1;
+    a.counters = d_misc_.as<unsigned int>();
+    const int grid = int(scratch_warps_ / kWarpsPerBlock);
+    const size_t smem = kWarpsPerBlock * kMaxSym * 32 * 8;
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    check_cuda(cudaMemsetAsync(a.counters, 0, 64, stream_), "memset counters");
+    nw_distance_kernel<<<grid, 32 * kWarpsPerBlock, smem, stream_>>>(a);
+    ++stats_.launches;
+    // level 0 tasks
+    a.tasks_out = d_tasks_[0].as<NwTask>();
+    a.tasks_out_cap = uint32_t(task_cap);
+    nw_root_tasks_kernel<<<int((n + 255) / 256), 256, 0, stream_>>>(a);
+    ++stats_.launches;
+    unsigned int h_cnt[4];
+    check_cuda(cudaMemcpyAsync(h_cnt, a.counters, 16, cudaMemcpyDeviceToHost, stream_), "D2H count");
+    check_cuda(cudaStreamSynchronize(stream_), "sync level");
+    if (h_cnt[2] != 0) throw Error{RB_ERR_DEVICE, "nw: distance kernel status " + std::to_string(h_cnt[2])};
+    uint32_t ntasks = h_cnt[1];
+    int cur = 0;
+    while (ntasks > 0) {
+        const size_t need = size_t(ntasks) * 2 + 64;
+        d_tasks_[cur ^ 1].reserve(need * sizeof(NwTask));
+        task_cap = d_tasks_[cur ^ 1].bytes / sizeof(NwTask);
+        a.tasks_in = d_tasks_[cur].as<NwTask>();
+        a.ntasks_in = ntasks;
+        a.tasks_out = d_tasks_[cur ^ 1].as<NwTask>();
+        a.tasks_out_cap = uint32_t(task_cap);
+        check_cuda(cudaMemsetAsync(a.counters, 0, 8, stream_), "memset counters");
+        nw_level_kernel<<<grid, 32 * kWarpsPerBlock, smem, stream_>>>(a);
+        ++stats_.launches;
+        check_cuda(cudaMemcpyAsync(h_cnt, a.counters, 16, cudaMemcpyDeviceToHost, stream_), "D2H count");
+        check_cuda(cudaStreamSynchronize(stream_), "sync level");
+        if (h_cnt[2] != 0) throw Error{RB_ERR_DEVICE, "nw: level kernel status " + std::to_string(h_cnt[2])};
+        ntasks = h_cnt[1];
+        cur ^= 1;
+    }
+    nw_breakpoints_kernel<<<int((n + 127) / 128), 128, 0, stream_>>>(a);
+    ++stats_.launches;
+    if (want_cigar_) {
+        d_ciglen_.reserve((n + 1) * sizeof(uint64_t));
+        d_cigoff_.reserve((n + 1) * sizeof(uint64_t));
+        nw_cigar_kernel<<<int((n + 127) / 128), 128, 0, stream_>>>(a, d_ciglen_.as<uint64_t>(), nullptr,
+                                                                   nullptr, 0);
+        exclusive_scan_kernel<<<1, 1024, 0, stream_>>>(d_ciglen_.as<uint64_t>(), d_cigoff_.as<uint64_t>(),
+                                                       uint32_t(n));
+        uint64_t total = 0;
+        check_cuda(cudaMemcpyAsync(&total, d_cigoff_.as<uint64_t>() + n, 8, cudaMemcpyDeviceToHost, stream_),
+                   "D2H cigar total");
+        check_cuda(cudaStreamSynchronize(stream_), "sync cigar");
+        d_cig_.reserve(std::max<uint64_t>(total, 1));
+        nw_cigar_kernel<<<int((n + 127) / 128), 128, 0, stream_>>>(a, d_ciglen_.as<uint64_t>(),
+                                                                   d_cigoff_.as<uint64_t>(), d_cig_.as<char>(), 1);
+        stats_.launches += 4;
+    }
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    check_cuda(cudaStreamSynchronize(stream_), "sync run");
+    check_cuda(cudaGetLastError(), "nw kernels");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.kernel_ms = ms;
+}
+
+
+void NwEngine::cigar_breakpoints(const rb_cigar_overlap* ovl, size_t n, uint32_t w, rb_aln_result* out) {
+    if (n > 0 && !ovl) throw Error{RB_ERR_ARG, "rb_cigar_breakpoints: overlaps is NULL"};
+    if (w == 0) throw Error{RB_ERR_ARG, "rb_cigar_breakpoints: window length is 0"};
+    uint64_t cbytes = 0, slots = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (ovl[i].t_end < ovl[i].t_begin || (ovl[i].cigar_length && !ovl[i].cigar))
+            throw Error{RB_ERR_ARG, "rb_cigar_breakpoints: invalid overlap"};
+        cbytes += ovl[i].cigar_length + 1;
+        const uint64_t segs = ovl[i].t_end > ovl[i].t_begin
+                                  ? (uint64_t(ovl[i].t_end) - 1) / w - ovl[i].t_begin / w + 1
+                                  : 1;
+        slots += 4 * segs;
+    }
+    h_codes_.reserve(std::max<uint64_t>(cbytes, 16));
+    h_pairs_.reserve(std::max<size_t>(n, 1) * sizeof(CigarOvlDev));
+    char* cb = h_codes_.as<char>();
+    CigarOvlDev* od = h_pairs_.as<CigarOvlDev>();
+    uint64_t off = 0, bo = 0;
+    for (size_t i = 0; i < n; ++i) {
+        od[i].cigar_off = off;
+        od[i].cigar_len = ovl[i].cigar_length;
+        od[i].q_offset = ovl[i].q_offset;
+        od[i].t_begin = ovl[i].t_begin;
+        od[i].t_end = ovl[i].t_end;
+        od[i].bp_off = bo;
+        if (ovl[i].cigar_length) memcpy(cb + off, ovl[i].cigar, ovl[i].cigar_length);
+        cb[off + ovl[i].cigar_length] = 0;
+        off += ovl[i].cigar_length + 1;
+        const uint64_t segs = ovl[i].t_end > ovl[i].t_begin
+                                  ? (uint64_t(ovl[i].t_end) - 1) / w - ovl[i].t_begin / w + 1
+                                  : 1;
+        bo += 4 * segs;
+    }
+    d_codes_.reserve(std::max<uint64_t>(off, 16));
+    d_pairs_.reserve(std::max<size_t>(n, 1) * sizeof(CigarOvlDev));
+    d_bp_.reserve(std::max<uint64_t>(slots, 1) * 4);
+    d_bpcnt_.reserve(std::max<size_t>(n, 1) * 4);
+    d_misc_.reserve(64);
+    check_cuda(cudaMemsetAsync(d_misc_.ptr, 0, 64, stream_), "memset status");
+    check_cuda(cudaMemcpyAsync(d_codes_.ptr, cb, off, cudaMemcpyHostToDevice, stream_), "H2D cigars");
+    check_cuda(cudaMemcpyAsync(d_pairs_.ptr, od, n * sizeof(CigarOvlDev), cudaMemcpyHostToDevice, stream_),
+               "H2D overlaps");
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    if (n)
+        cigar_breakpoints_kernel<<<int((n + 127) / 128), 128, 0, stream_>>>(
+            d_codes_.as<char>(), d_pairs_.as<CigarOvlDev>(), uint32_t(n), w, d_bp_.as<uint32_t>(),
+            d_bpcnt_.as<uint32_t>(), d_misc_.as<unsigned int>());
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    std::vector<uint32_t> cnt(n), raw(slots);
+    unsigned int status = 0;
+    if (n) {
+        check_cuda(cudaMemcpyAsync(cnt.data(), d_bpcnt_.ptr, n * 4, cudaMemcpyDeviceToHost, stream_), "D2H");
+        check_cuda(cudaMemcpyAsync(raw.data(), d_bp_.ptr, slots * 4, cudaMemcpyDeviceToHost, stream_), "D2H");
+    }
+    check_cuda(cudaMemcpyAsync(&status, d_misc_.ptr, 4, cudaMemcpyDeviceToHost, stream_), "D2H");
+    check_cuda(cudaStreamSynchronize(stream_), "sync cigar breakpoints");
+    check_cuda(cudaGetLastError(), "cigar breakpoints kernel");
+    if (status) throw Error{RB_ERR_ARG, "rb_cigar_breakpoints: CIGAR runs past the target span"};
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.kernel_ms = ms;
+    stats_.launches = n ? 1 : 0;
+    stats_.items = n;
+    npairs_ = 0;
+    dist_.assign(n, -1);
+    bp_offsets_.assign(n + 1, 0);
+    bp_.clear();
+    for (size_t i = 0; i < n; ++i) {
+        bp_offsets_[i] = bp_.size();
+        bp_.insert(bp_.end(), raw.begin() + od[i].bp_off, raw.begin() + od[i].bp_off + cnt[i]);
+    }
+    bp_offsets_[n] = bp_.size();
+    out->edit_distance = dist_.data();
+    out->breakpoints = bp_.data();
+    out->bp_offsets = bp_offsets_.data();
+    out->cigars = nullptr;
+    out->cigar_offsets = nullptr;
+}
+
+void NwEngine::fetch(rb_aln_result* out) {
+    const size_t n = npairs_;
+    check_cuda(cudaEventRecord(ev2_, stream_), "cudaEventRecord");
+    dist_.resize(n);
+    std::vector<uint32_t> cnt(n);
+    std::vector<uint32_t> raw(bp_slots_);
+    if (n) {
+        check_cuda(cudaMemcpyAsync(dist_.data(), d_dist_.ptr, n * 4, cudaMemcpyDeviceToHost, stream_), "D2H dist");
+        check_cuda(cudaMemcpyAsync(cnt.data(), d_bpcnt_.ptr, n * 4, cudaMemcpyDeviceToHost, stream_), "D2H bpcnt");
+        if (bp_slots_)
+            check_cuda(cudaMemcpyAsync(raw.data(), d_bp_.ptr, bp_slots_ * 4, cudaMemcpyDeviceToHost, stream_),
+                       "D2H bp");
+    }
+    uint64_t d2h = n * 8 + bp_slots_ * 4;
+    std::vector<uint64_t> cigoff;
+    if (want_cigar_ && n) {
+        cigoff.resize(n + 1);
+        check_cuda(cudaMemcpyAsync(cigoff.data(), d_cigoff_.ptr, (n + 1) * 8, cudaMemcpyDeviceToHost, stream_),
+                   "D2H cigoff");
+        check_cuda(cudaStreamSynchronize(stream_), "sync fetch");
+        cig_.resize(cigoff[n]);
+        if (cigoff[n])
+            check_cuda(cudaMemcpyAsync(cig_.data(), d_cig_.ptr, cigoff[n], cudaMemcpyDeviceToHost, stream_),
+                       "D2H cigars");
+        d2h += (n + 1) * 8 + cigoff[n];
+    }
+    check_cuda(cudaEventRecord(ev3_, stream_), "cudaEventRecord");
+    check_cuda(cudaStreamSynchronize(stream_), "sync fetch");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev2_, ev3_);
+    stats_.d2h_ms = ms;
+    stats_.d2h_bytes = d2h;
+    // compact breakpoints
+    const NwPairDev* pd = h_pairs_.as<NwPairDev>();
+    bp_offsets_.assign(n + 1, 0);
+    bp_.clear();
+    for (size_t i = 0; i < n; ++i) {
+        bp_offsets_[i] = bp_.size();
+        bp_.insert(bp_.end(), raw.begin() + pd[i].bp_off, raw.begin() + pd[i].bp_off + cnt[i]);
+    }
+    bp_offsets_[n] = bp_.size();
+    out->edit_distance = dist_.data();
+    out->breakpoints = bp_.data();
+    out->bp_offsets = bp_offsets_.data();
+    if (want_cigar_) {
+        cig_offsets_ = cigoff.empty() ? std::vector<uint64_t>(n + 1, 0) : cigoff;
+        out->cigars = cig_.data();
+        out->cigar_offsets = cig_offsets_.data();
+    } else {
+        out->cigars = nullptr;
+        out->cigar_offsets = nullptr;
+    }
+}
+
+}  // namespace rb

@@ -1,0 +1,209 @@
+// C ABI of racon_b200 (declared in include/racon_b200.h). Thin layer over the
+// device engines: argument checks, device selection, error codes.
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "../../include/racon_b200.h"
+#include "rb_internal.hpp"
+
+namespace rb {
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        const int code = (e == cudaErrorMemoryAllocation) ? RB_ERR_NOMEM : RB_ERR_CUDA;
+        throw Error{code, std::string(what) + ": " + cudaGetErrorString(e)};
+    }
+}
+
+void DevBuf::reserve(size_t need) {
+    if (need <= bytes && ptr) return;
+    release();
+    size_t b = need < 256 ? 256 : need;
+    check_cuda(cudaMalloc(&ptr, b), "cudaMalloc");
+    bytes = b;
+}
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+void HostBuf::reserve(size_t need) {
+    if (need <= bytes && ptr) return;
+    release();
+    size_t b = need < 256 ? 256 : need;
+    b = b + b / 4;  // headroom for growing batches
+    check_cuda(cudaMallocHost(&ptr, b), "cudaMallocHost");
+    bytes = b;
+}
+void HostBuf::release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+}  // namespace rb
+
+struct rb_ctx {
+    rb::DeviceInfo dev;
+    cudaStream_t stream = nullptr;
+    rb_params params{};
+    std::unique_ptr<rb::NwEngine> nw;
+    std::unique_ptr<rb::PoaEngine> poa;
+    std::string err;
+};
+
+namespace {
+std::mutex g_err_mu;
+std::string g_create_err;
+
+void set_create_error(const std::string& s) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_create_err = s;
+}
+
+template <class F>
+int guarded(rb_ctx* ctx, F&& f) {
+    if (!ctx) return RB_ERR_ARG;
+    try {
+        cudaSetDevice(ctx->dev.device);
+        f();
+        ctx->err.clear();
+        return RB_OK;
+    } catch (const rb::Error& e) {
+        ctx->err = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        ctx->err = "host allocation failed";
+        return RB_ERR_NOMEM;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+rb_ctx* rb_create(int device, const rb_params* params) {
+    if (!params) {
+        set_create_error("rb_create: params is NULL");
+        return nullptr;
+    }
+    if (params->window_length == 0) {
+        set_create_error("rb_create: invalid window length");
+        return nullptr;
+    }
+    if (params->gap > 0) {
+        set_create_error("rb_create: gap penalty must be non-positive");
+        return nullptr;
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) {
+        set_create_error("rb_create: no CUDA device");
+        return nullptr;
+    }
+    if (device < 0 || device >= count) {
+        set_create_error("rb_create: device index out of range");
+        return nullptr;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        set_create_error("rb_create: cudaGetDeviceProperties failed");
+        return nullptr;
+    }
+    if (prop.major != 10) {
+        set_create_error("rb_create: device is not sm_100 (B200); this build carries sm_100a code only");
+        return nullptr;
+    }
+    auto ctx = std::unique_ptr<rb_ctx>(new rb_ctx());
+    ctx->dev.device = device;
+    ctx->dev.sm_count = prop.multiProcessorCount;
+    ctx->dev.smem_optin = prop.sharedMemPerBlockOptin;
+    ctx->params = *params;
+    try {
+        rb::check_cuda(cudaSetDevice(device), "cudaSetDevice");
+        rb::check_cuda(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ctx->nw.reset(new rb::NwEngine(ctx->dev, ctx->stream));
+        ctx->poa.reset(new rb::PoaEngine(ctx->dev, ctx->stream, params->match, params->mismatch, params->gap));
+    } catch (const rb::Error& e) {
+        set_create_error(e.msg);
+        return nullptr;
+    }
+    return ctx.release();
+}
+
+const char* rb_create_error(void) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    return g_create_err.c_str();
+}
+
+void rb_destroy(rb_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->dev.device);
+    ctx->nw.reset();
+    ctx->poa.reset();
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* rb_last_error(const rb_ctx* ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
+
+int rb_align_stage(rb_ctx* ctx, const rb_pair* pairs, size_t n, int want_cigar) {
+    return guarded(ctx, [&]() { ctx->nw->stage(pairs, n, want_cigar, ctx->params.window_length); });
+}
+int rb_align_run(rb_ctx* ctx) {
+    return guarded(ctx, [&]() { ctx->nw->run(); });
+}
+int rb_align_fetch(rb_ctx* ctx, rb_aln_result* out) {
+    if (!out) return RB_ERR_ARG;
+    return guarded(ctx, [&]() { ctx->nw->fetch(out); });
+}
+int rb_align_batch(rb_ctx* ctx, const rb_pair* pairs, size_t n, int want_cigar, rb_aln_result* out) {
+    if (!out) return RB_ERR_ARG;
+    return guarded(ctx, [&]() {
+        ctx->nw->stage(pairs, n, want_cigar, ctx->params.window_length);
+        ctx->nw->run();
+        ctx->nw->fetch(out);
+    });
+}
+
+int rb_cigar_breakpoints(rb_ctx* ctx, const rb_cigar_overlap* overlaps, size_t n, rb_aln_result* out) {
+    if (!out) return RB_ERR_ARG;
+    return guarded(ctx, [&]() { ctx->nw->cigar_breakpoints(overlaps, n, ctx->params.window_length, out); });
+}
+
+int rb_poa_stage(rb_ctx* ctx, const rb_window* windows, size_t n, int trim) {
+    return guarded(ctx, [&]() { ctx->poa->stage(windows, n, trim); });
+}
+int rb_poa_run(rb_ctx* ctx) {
+    return guarded(ctx, [&]() { ctx->poa->run(); });
+}
+int rb_poa_fetch(rb_ctx* ctx, rb_poa_result* out) {
+    if (!out) return RB_ERR_ARG;
+    return guarded(ctx, [&]() { ctx->poa->fetch(out); });
+}
+int rb_poa_batch(rb_ctx* ctx, const rb_window* windows, size_t n, int trim, rb_poa_result* out) {
+    if (!out) return RB_ERR_ARG;
+    return guarded(ctx, [&]() {
+        ctx->poa->stage(windows, n, trim);
+        ctx->poa->run();
+        ctx->poa->fetch(out);
+    });
+}
+
+int rb_poa_stats(const rb_ctx* ctx, rb_stats* out) {
+    if (!ctx || !out) return RB_ERR_ARG;
+    *out = ctx->poa->stats();
+    return RB_OK;
+}
+int rb_align_stats(const rb_ctx* ctx, rb_stats* out) {
+    if (!ctx || !out) return RB_ERR_ARG;
+    *out = ctx->nw->stats();
+    return RB_OK;
+}
+
+void rb_free(void* p) { free(p); }
+
+}  // extern "C"

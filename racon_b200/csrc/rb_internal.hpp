@@ -1,0 +1,124 @@
+// Internal host-side interfaces shared by the C ABI (rb_capi.cpp) and the
+// device engines (nw_align.cu, poa_consensus.cu). Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/racon_b200.h"
+
+namespace rb {
+
+// Error with an RB_ERR_* code; thrown inside the library, turned into a
+// return code at the C ABI boundary.
+struct Error {
+    int code;
+    std::string msg;
+};
+
+void check_cuda(cudaError_t e, const char* what);
+
+// Growable device buffer (cudaMalloc'd, reused across calls).
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t need);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+    ~DevBuf() { release(); }
+};
+
+// Growable pinned host buffer.
+struct HostBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t need);
+    void release();
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+    ~HostBuf() { release(); }
+};
+
+struct DeviceInfo {
+    int device = 0;
+    int sm_count = 148;
+    size_t smem_optin = 0;
+};
+
+// ----- overlap alignment engine (nw_align.cu) -----
+struct NwPairDev {
+    uint64_t q_off, t_off;  // offsets of the encoded query / target in the code buffer
+    uint64_t mq_off;        // offset of the per-target-position match array
+    uint64_t bp_off;        // offset (uint32 units) of the breakpoint slots
+    uint32_t m, n;          // query / target span lengths
+    uint32_t nsym;          // symbol codes are < nsym
+    uint32_t q_offset, t_begin;
+};
+
+class NwEngine {
+public:
+    explicit NwEngine(const DeviceInfo& dev, cudaStream_t stream);
+    ~NwEngine();
+    void stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t window_length);
+    void run();
+    void fetch(rb_aln_result* out);
+    // breaking points straight from SAM CIGARs (no alignment)
+    void cigar_breakpoints(const rb_cigar_overlap* ovl, size_t n, uint32_t window_length,
+                           rb_aln_result* out);
+    const rb_stats& stats() const { return stats_; }
+
+private:
+    void reserve_scratch(uint32_t max_m, uint32_t max_n);
+    DeviceInfo dev_;
+    cudaStream_t stream_;
+    cudaEvent_t ev0_, ev1_, ev2_, ev3_;
+    size_t npairs_ = 0;
+    int want_cigar_ = 0;
+    uint32_t window_length_ = 500;
+    uint32_t max_m_ = 0, max_n_ = 0;
+    uint64_t code_bytes_ = 0, mq_len_ = 0, bp_slots_ = 0;
+    HostBuf h_codes_, h_pairs_, h_order_;
+    HostBuf h_dist_, h_bp_, h_bpcnt_, h_cig_, h_cigoff_, h_misc_;
+    DevBuf d_codes_, d_pairs_, d_order_, d_dist_, d_mq_, d_bp_, d_bpcnt_;
+    DevBuf d_tasks_[2], d_misc_, d_scratch_, d_ciglen_, d_cigoff_, d_cig_;
+    size_t scratch_warps_ = 0, scratch_stride_ = 0;
+    std::vector<int32_t> dist_;
+    std::vector<uint64_t> bp_offsets_, cig_offsets_;
+    std::vector<uint32_t> bp_;
+    std::vector<char> cig_;
+    rb_stats stats_{};
+};
+
+// ----- window consensus engine (poa_consensus.cu) -----
+class PoaEngine {
+public:
+    PoaEngine(const DeviceInfo& dev, cudaStream_t stream, int8_t m, int8_t x, int8_t g);
+    ~PoaEngine();
+    void stage(const rb_window* wins, size_t n, int trim);
+    void run();
+    void fetch(rb_poa_result* out);
+    const rb_stats& stats() const { return stats_; }
+
+private:
+    DeviceInfo dev_;
+    cudaStream_t stream_;
+    cudaEvent_t ev0_, ev1_, ev2_, ev3_;
+    int8_t match_, mismatch_, gap_;
+    int trim_ = 1;
+    size_t nwin_ = 0;
+    uint64_t in_bytes_ = 0, out_cap_ = 0;
+    uint32_t max_len_ = 0, max_nodes_cap_ = 0;
+    HostBuf h_in_, h_desc_, h_layers_, h_order_, h_out_, h_outlen_, h_flags_;
+    DevBuf d_in_, d_desc_, d_layers_, d_order_, d_out_, d_outlen_, d_flags_, d_misc_;
+    DevBuf d_graph_, d_dp_;
+    size_t slots_ = 0, graph_stride_ = 0, dp_stride_ = 0;
+    std::vector<uint64_t> offsets_;
+    std::vector<char> cons_;
+    std::vector<uint8_t> polished_;
+    std::vector<std::pair<uint64_t, uint32_t>> labels_;  // (id, rank) per window
+    rb_stats stats_{};
+};
+
+}  // namespace rb
