@@ -200,6 +200,21 @@ int rb_polish_files(const char* sequences_path, const char* overlaps_path,
                     int8_t match, int8_t mismatch, int8_t gap, uint32_t threads,
                     int drop_unpolished, int device, char** fasta, double* stage_seconds);
 const char* rb_pipeline_error(void);
+
+/* A polishing job stopped after racon's initialize() (src/polisher.cpp:192-460:
+ * loading, overlap filtering, device alignment + breaking points, windows
+ * and layers). rb_job_windows exposes its windows, in racon's window order,
+ * as rb_window views valid until rb_job_free; they can be passed directly to
+ * rb_poa_batch / rb_poa_stage. stage_seconds (may be NULL) receives load,
+ * align and layer-assembly wall seconds. Returns NULL on error
+ * (rb_pipeline_error() holds the message). */
+typedef struct rb_job rb_job;
+rb_job* rb_job_prepare(const char* sequences_path, const char* overlaps_path,
+                       const char* target_path, int fragment, uint32_t window_length,
+                       double quality_threshold, double error_threshold, int8_t match,
+                       int8_t mismatch, int8_t gap, int device, double* stage_seconds);
+size_t rb_job_windows(const rb_job* job, const rb_window** windows);
+void rb_job_free(rb_job* job);
 void rb_free(void* p);
 
 #ifdef __cplusplus

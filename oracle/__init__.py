@@ -48,6 +48,9 @@ def load():
     lib.oracle_dump_windows.argtypes = [c.c_char_p] * 3 + [c.c_int, c.c_uint32, c.c_double, c.c_double,
                                                            c.c_uint32, c.POINTER(c.c_uint64)]
     lib.oracle_free.argtypes = [c.c_void_p]
+    lib.oracle_consensus_blob.restype = c.c_int64
+    lib.oracle_consensus_blob.argtypes = [c.c_char_p, c.c_uint64, c.c_int64, c.c_uint32, c.c_int, c.c_int, c.c_int,
+                                          c.c_int, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
     _lib = lib
     return lib
 
@@ -163,3 +166,34 @@ def dump_windows(sequences, overlaps, targets, fragment=False, window_length=500
         wins.append({"id": tid, "rank": rank, "tgs": tgs, "backbone": bb, "backbone_quality": bq,
                      "layers": layers, "qualities": quals, "begins": begins, "ends": ends})
     return wins
+
+
+def windows_blob(windows):
+    """Windows (dicts) in the oracle_dump_windows layout."""
+    parts = [struct.pack("<Q", len(windows))]
+    for w in windows:
+        bb = _b(w["backbone"])
+        bq = _b(w.get("backbone_quality")) or b"!" * len(bb)
+        parts.append(struct.pack("<QIBII", w.get("id", 0), w.get("rank", 0), int(w.get("tgs", 1)), len(bb),
+                                 len(w["layers"])))
+        parts += [bb, bq]
+        quals = w.get("qualities") or [None] * len(w["layers"])
+        for s_, q, b, e in zip(w["layers"], quals, w["begins"], w["ends"]):
+            s_ = _b(s_)
+            parts.append(struct.pack("<IIIB", len(s_), b, e, 1 if q else 0))
+            parts.append(s_)
+            if q:
+                parts.append(_b(q))
+    return b"".join(parts)
+
+
+def consensus_blob(blob, max_windows, threads, match, mismatch, gap, trim=True):
+    """CPU window consensus of up to max_windows windows on `threads` threads:
+    (windows done, seconds, DP cells)."""
+    sec = ctypes.c_double()
+    cells = ctypes.c_uint64()
+    n = load().oracle_consensus_blob(blob, len(blob), max_windows, threads, match, mismatch, gap, int(trim),
+                                     ctypes.byref(sec), ctypes.byref(cells))
+    if n < 0:
+        raise RuntimeError("bad window blob")
+    return n, sec.value, cells.value

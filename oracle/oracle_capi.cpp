@@ -187,3 +187,77 @@ char* oracle_dump_windows(const char* sequences, const char* overlaps, const cha
 }
 
 }  // extern "C"
+
+#include <atomic>
+#include <chrono>
+#include <thread>
+
+extern "C" {
+
+// Window consensus of the first max_windows windows of a blob in the
+// oracle_dump_windows layout, on `threads` host threads. Returns the number of
+// windows done; *seconds = wall time of the consensus loop, *cells = DP cells.
+// Used as the CPU baseline (the oracle, not reference racon).
+int64_t oracle_consensus_blob(const char* blob, uint64_t nbytes, int64_t max_windows, uint32_t threads,
+                              int match, int mismatch, int gap, int trim, double* seconds,
+                              uint64_t* cells) {
+    uint64_t off = 0;
+    auto get = [&](void* dst, size_t n) {
+        if (off + n > nbytes) return false;
+        memcpy(dst, blob + off, n);
+        off += n;
+        return true;
+    };
+    uint64_t nw = 0;
+    if (!get(&nw, 8)) return -1;
+    std::vector<CpuWindowInput> wins;
+    std::vector<uint8_t> tgs;
+    for (uint64_t i = 0; i < nw && int64_t(wins.size()) < max_windows; ++i) {
+        uint64_t tid;
+        uint32_t rank, bl, nl;
+        uint8_t t;
+        if (!get(&tid, 8) || !get(&rank, 4) || !get(&t, 1) || !get(&bl, 4) || !get(&nl, 4)) return -1;
+        CpuWindowInput w;
+        w.backbone = blob + off;
+        w.backbone_len = bl;
+        off += bl;
+        w.backbone_qual = blob + off;
+        off += bl;
+        for (uint32_t k = 0; k < nl; ++k) {
+            uint32_t len, b, e;
+            uint8_t hq;
+            if (!get(&len, 4) || !get(&b, 4) || !get(&e, 4) || !get(&hq, 1)) return -1;
+            w.seqs.push_back(blob + off);
+            off += len;
+            w.quals.push_back(hq ? blob + off : nullptr);
+            if (hq) off += len;
+            w.lens.push_back(len);
+            w.positions.emplace_back(b, e);
+        }
+        if (off > nbytes) return -1;
+        wins.push_back(std::move(w));
+        tgs.push_back(t);
+    }
+    std::vector<uint64_t> c(wins.size(), 0);
+    std::atomic<size_t> next(0);
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (uint32_t k = 0; k < std::max<uint32_t>(1, threads); ++k) {
+        pool.emplace_back([&]() {
+            for (size_t i = next++; i < wins.size(); i = next++) {
+                std::string cons;
+                WindowStats st;
+                window_consensus(wins[i], tgs[i] != 0, trim != 0, match, mismatch, gap, cons, &st);
+                c[i] = st.cells;
+            }
+        });
+    }
+    for (auto& th : pool) th.join();
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    uint64_t total = 0;
+    for (auto x : c) total += x;
+    *cells = total;
+    return int64_t(wins.size());
+}
+
+}  // extern "C"

@@ -118,6 +118,13 @@ def load():
                                     ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                     ctypes.POINTER(ctypes.c_double)]
     lib.rb_pipeline_error.restype = ctypes.c_char_p
+    lib.rb_job_prepare.restype = vp
+    lib.rb_job_prepare.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint32,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_int8, ctypes.c_int8, ctypes.c_int8,
+                                   ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.rb_job_windows.restype = ctypes.c_size_t
+    lib.rb_job_windows.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(_Window))]
+    lib.rb_job_free.argtypes = [vp]
     lib.rb_free.argtypes = [vp]
     _lib = lib
     return lib
@@ -268,6 +275,17 @@ class Context:
         self._check(self.lib.rb_poa_fetch(self.ptr, ctypes.byref(r)))
         return self._poa_out(r, self._staged_windows)
 
+    def poa_job(self, job, trim=True):
+        """Consensus of every window of a Job, passing its window views straight
+        to rb_poa_batch (host buffers, copies included)."""
+        r = _PoaResult()
+        self._check(self.lib.rb_poa_batch(self.ptr, job.windows, job.n, int(trim), ctypes.byref(r)))
+        return self._poa_out(r, job.n)
+
+    def poa_stage_job(self, job, trim=True):
+        self._check(self.lib.rb_poa_stage(self.ptr, job.windows, job.n, int(trim)))
+        self._staged_windows = job.n
+
     def poa_stats(self):
         s = Stats()
         self._check(self.lib.rb_poa_stats(self.ptr, ctypes.byref(s)))
@@ -298,3 +316,61 @@ def polish_files(sequences, overlaps, targets, fragment=False, window_length=500
     if stage_seconds is not None:
         stage_seconds[:] = list(st)
     return text
+
+
+class Job:
+    """racon's initialize() with the device aligner (rb_job_prepare): loading,
+    overlap filtering, breaking points, windows and layers. .windows / .n are
+    the rb_window views of every window, in racon's order."""
+
+    def __init__(self, sequences, overlaps, targets, fragment=False, window_length=500, quality_threshold=10.0,
+                 error_threshold=0.3, match=3, mismatch=-5, gap=-4, device=0):
+        self.lib = load()
+        st = (ctypes.c_double * 3)()
+        self.ptr = self.lib.rb_job_prepare(_b(sequences), _b(overlaps), _b(targets), int(fragment), window_length,
+                                           quality_threshold, error_threshold, match, mismatch, gap, device, st)
+        if not self.ptr:
+            raise RaconB200Error(1, self.lib.rb_pipeline_error().decode())
+        self.stage_seconds = list(st)
+        wp = ctypes.POINTER(_Window)()
+        self.n = self.lib.rb_job_windows(self.ptr, ctypes.byref(wp))
+        self.windows = wp
+
+    def close(self):
+        if self.ptr:
+            self.lib.rb_job_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def window(self, i):
+        """Window i as a dict (backbone, backbone_quality, layers, qualities,
+        begins, ends, tgs, id, rank)."""
+        w = self.windows[i]
+        bl = w.backbone_length
+        bb = ctypes.string_at(w.backbone, bl)
+        bq = ctypes.string_at(w.backbone_quality, bl) if w.backbone_quality else None
+        layers, quals, begins, ends = [], [], [], []
+        for j in range(w.n_layers):
+            ln = w.layer_lengths[j]
+            layers.append(ctypes.string_at(w.layers[j], ln))
+            q = w.layer_qualities[j] if w.layer_qualities else None
+            quals.append(ctypes.string_at(q, ln) if q else None)
+            begins.append(w.begins[j])
+            ends.append(w.ends[j])
+        return {"backbone": bb, "backbone_quality": bq, "layers": layers, "qualities": quals, "begins": begins,
+                "ends": ends, "tgs": w.tgs, "id": w.id, "rank": w.rank}
+
+    def layer_stats(self):
+        """(windows, layers, layer bases, backbone bases)."""
+        nl = lb = bb = 0
+        for i in range(self.n):
+            w = self.windows[i]
+            nl += w.n_layers
+            bb += w.backbone_length
+            lb += sum(w.layer_lengths[j] for j in range(w.n_layers))
+        return self.n, nl, lb, bb

@@ -820,3 +820,69 @@ extern "C" int rb_polish_files(const char* sequences_path, const char* overlaps_
         return RB_ERR_ARG;
     }
 }
+
+// ---------------------------------------------------------------- jobs
+
+struct rb_job {
+    std::unique_ptr<racon::Polisher> polisher;
+    std::vector<rb_window> views;
+    double stage_s[3] = {0, 0, 0};
+
+    // window views after initialize() (friend of racon::Polisher)
+    void collect() {
+        const racon::Polisher& p = *polisher;
+        views.resize(p.windows_.size());
+        for (size_t i = 0; i < p.windows_.size(); ++i) {
+            const racon::Window& w = *p.windows_[i];
+            rb_window& r = views[i];
+            r.backbone = w.backbone;
+            r.backbone_quality = w.quality;
+            r.backbone_length = w.backbone_length;
+            r.n_layers = uint32_t(w.seqs.size());
+            r.layers = w.seqs.data();
+            r.layer_qualities = w.quals.data();
+            r.layer_lengths = w.lens.data();
+            r.begins = w.begins.data();
+            r.ends = w.ends.data();
+            r.tgs = p.tgs_ ? 1 : 0;
+            r.id = w.id;
+            r.rank = w.rank;
+        }
+        for (int i = 0; i < 3; ++i) stage_s[i] = p.stage_s_[i];
+    }
+};
+
+extern "C" rb_job* rb_job_prepare(const char* sequences_path, const char* overlaps_path, const char* target_path,
+                                  int fragment, uint32_t window_length, double quality_threshold,
+                                  double error_threshold, int8_t match, int8_t mismatch, int8_t gap, int device,
+                                  double* stage_seconds) {
+    if (!sequences_path || !overlaps_path || !target_path) return nullptr;
+    racon::g_throw_on_error = true;
+    std::string dev = std::to_string(device);
+    setenv("RACON_B200_DEVICE", dev.c_str(), 1);
+    try {
+        std::unique_ptr<rb_job> job(new rb_job());
+        job->polisher = racon::createPolisher(sequences_path, overlaps_path, target_path,
+                                              fragment ? racon::PolisherType::kF : racon::PolisherType::kC,
+                                              window_length, quality_threshold, error_threshold, true, match,
+                                              mismatch, gap, 1);
+        job->polisher->initialize();
+        job->collect();
+        if (stage_seconds)
+            for (int i = 0; i < 3; ++i) stage_seconds[i] = job->stage_s[i];
+        racon::g_throw_on_error = false;
+        return job.release();
+    } catch (const racon::Fatal& e) {
+        racon::g_throw_on_error = false;
+        g_pipeline_error = e.what();
+        return nullptr;
+    }
+}
+
+extern "C" size_t rb_job_windows(const rb_job* job, const rb_window** windows) {
+    if (!job || !windows) return 0;
+    *windows = job->views.data();
+    return job->views.size();
+}
+
+extern "C" void rb_job_free(rb_job* job) { delete job; }

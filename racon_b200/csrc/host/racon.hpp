@@ -18,6 +18,7 @@
 #include <vector>
 
 struct rb_ctx;
+struct rb_job;
 
 namespace racon {
 
@@ -88,6 +89,7 @@ public:
         double error_threshold, bool trim, int8_t match, int8_t mismatch, int8_t gap,
         uint32_t num_threads, uint32_t cuda_batches, bool cuda_banded_alignment,
         uint32_t cudaaligner_batches, uint32_t cudaaligner_band_width);
+    friend struct ::rb_job;
 
 protected:
     Polisher(const std::string& sequences_path, const std::string& overlaps_path,

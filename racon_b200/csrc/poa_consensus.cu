@@ -29,6 +29,7 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <numeric>
 
 #include "rb_internal.hpp"
@@ -1116,6 +1117,9 @@ void PoaEngine::run() {
         const size_t slot = walk_layout(ncap, ecap, acap, lcap, [](int, size_t) {});
         const size_t budget = size_t(24) << 30;
         size_t slots = std::min<size_t>(todo.size(), size_t(dev_.sm_count) * 4);
+        // RB_POA_SLOTS caps the resident windows (smaller scratch, e.g. for
+        // profiler captures); results do not depend on it
+        if (const char* e = getenv("RB_POA_SLOTS")) slots = std::max<size_t>(1, std::min<size_t>(slots, strtoull(e, nullptr, 10)));
         while (slots > 1 && slots * slot > budget) slots /= 2;
         d_graph_.reserve(slots * slot);
         d_order_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
