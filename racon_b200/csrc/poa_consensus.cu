@@ -37,8 +37,8 @@
 namespace rb {
 namespace {
 
-constexpr int kPoaThreads = 128;
-constexpr int kNegInf = -1000000000;
+// minus infinity that survives thousands of gap additions without overflow
+constexpr int kNegInf = -(1 << 29);
 constexpr uint64_t kNoQual = ~0ull;
 
 enum PoaFlag : uint8_t {
@@ -96,10 +96,14 @@ struct Graph {
     int *a_node, *a_next;
     int* stack;
     int *pred_off, *pred_idx;
+    int4* rowdesc;  // per DP row: first three predecessor ranks (or the list offset) | count, sink, base
     int *aln_node, *aln_pos;
     long long* bscore;
     int* bpred;
     int* cons;
+    // valid topological order kept incrementally (rank -> node, node -> rank),
+    // its double buffer, per-rank shift counts and the new nodes of a layer
+    int *ord, *ord2, *my_rank, *shift, *nw_node, *nw_slot;
     int* H;
     uint8_t* dec;
     int ncap, ecap, acap, scap, lcap, alncap;
@@ -153,13 +157,20 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(N * 4, 30);       // cons
     take((N + 1) * L * 4, 31);  // H
     take((N + 1) * L, 32);      // dec
+    take(N * 4, 33);       // ord
+    take(N * 4, 34);       // ord2
+    take(N * 4, 35);       // my_rank
+    take((N + 2) * 4, 36); // shift
+    take(N * 4, 37);       // nw_node
+    take(N * 4, 38);       // nw_slot
+    take((N + 32) * 16, 39);  // rowdesc
     return off;
 }
 
 __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
     uint8_t* base = a.scratch + size_t(slot) * a.slot_bytes;
     Graph g;
-    void* p[33];
+    void* p[40];
     walk_layout(a.ncap, a.ecap, a.acap, a.lcap, [&](int id, size_t off) { p[id] = base + off; });
     g.code = (uint8_t*)p[0];
     g.cov = (uint32_t*)p[1];
@@ -194,6 +205,13 @@ __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
     g.cons = (int*)p[30];
     g.H = (int*)p[31];
     g.dec = (uint8_t*)p[32];
+    g.ord = (int*)p[33];
+    g.ord2 = (int*)p[34];
+    g.my_rank = (int*)p[35];
+    g.shift = (int*)p[36];
+    g.nw_node = (int*)p[37];
+    g.nw_slot = (int*)p[38];
+    g.rowdesc = (int4*)p[39];
     g.ncap = a.ncap;
     g.ecap = a.ecap;
     g.acap = a.acap;
@@ -204,18 +222,20 @@ __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
 }
 
 // Shared per-CTA state.
+// NW end cell of one layer: first sink row (in the DP order) with the best
+// last-column value, that value, and how many sinks share it.
+struct EndCell {
+    int row, value, ties;
+};
+
 struct PoaShared {
     int nnodes, nedges, naligned, nseq;
+    int nnew;     // new nodes of the last insertion (g.nw_node / g.nw_slot)
     int nranks;   // entries of rank_to_node (full graph order)
     int ndp;      // rows of the current DP
     int fail;     // 0 ok, else PoaFlag
     int iend;     // DP rank of the NW end cell
     int naln;
-    int best_val, best_rank;
-    int scan_v[kPoaThreads / 32];
-    int scan_l[kPoaThreads / 32];
-    int red_v[kPoaThreads / 32];
-    int red_r[kPoaThreads / 32];
 };
 
 // ---------------- graph primitives (thread 0) ----------------
@@ -355,12 +375,40 @@ __device__ bool g_mark_subgraph(const Graph& g, PoaShared& sh, int begin_node, i
 
 __device__ int layer_weight(const uint8_t* qual, int k) { return qual ? int(qual[k]) - 33 : 1; }
 
+// Rank extent, in the incremental order, of the aligned group of an existing
+// node v among the nodes that existed before this insertion (ids < nold).
+__device__ int group_end_rank(const Graph& g, int v, int nold) {
+    int r = g.my_rank[v];
+    for (int x = g.al_head[v]; x != -1; x = g.a_next[x]) {
+        const int y = g.a_node[x];
+        if (y < nold) r = max(r, g.my_rank[y]);
+    }
+    return r;
+}
+__device__ int group_start_rank(const Graph& g, int v, int nold) {
+    int r = g.my_rank[v];
+    for (int x = g.al_head[v]; x != -1; x = g.a_next[x]) {
+        const int y = g.a_node[x];
+        if (y < nold) r = min(r, g.my_rank[y]);
+    }
+    return r;
+}
+
+constexpr int kPendingSlot = INT_MIN;
+
 // Graph::add_alignment for one layer (alignment in g.aln_* reversed order,
-// entries [0, naln) from the end of the path back to its start).
+// entries [0, naln) from the end of the path back to its start). Also lists
+// the new nodes in path order with the rank slot of the old order after which
+// each one goes (g.nw_node / g.nw_slot, sh.nnew): head nodes before the
+// aligned group of the first existing node on the path, a node joining an
+// aligned group right after that group, every other new node after the
+// previous node on the path. The slots are non-decreasing along the path.
 __device__ void g_add_alignment(const Graph& g, PoaShared& sh, const uint8_t* seq, const uint8_t* qual,
                                 int len) {
+    sh.nnew = 0;
     if (len == 0) return;
     const int naln = sh.naln;
+    const int nold = sh.nnodes;
     const bool count_cov = len >= 2;
     int first_pos = -1, last_pos = -1;
     for (int k = naln - 1; k >= 0; --k) {
@@ -373,24 +421,28 @@ __device__ void g_add_alignment(const Graph& g, PoaShared& sh, const uint8_t* se
         sh.fail = kFailed;
         return;
     }
+    int nnew = 0;
     // head part [0, first_pos), then tail part (last_pos, len)
-    int head = -1, begin_id = -1;
+    int head = -1;
     for (int k = 0; k < first_pos; ++k) {
         const int id = g_add_node(g, sh, seq[k]);
         if (id < 0) return;
         if (count_cov) g.cov[id] += 1;
         if (k > 0) g_add_edge(g, sh, id - 1, id, layer_weight(qual, k - 1) + layer_weight(qual, k));
-        if (begin_id == -1) begin_id = id;
         head = id;
+        g.nw_node[nnew] = id;
+        g.nw_slot[nnew++] = kPendingSlot;
     }
-    int tail = -1;
+    int tail = -1, tail_first = -1, tail_count = 0;
     for (int k = last_pos + 1; k < len; ++k) {
         const int id = g_add_node(g, sh, seq[k]);
         if (id < 0) return;
         if (count_cov) g.cov[id] += 1;
         if (k > last_pos + 1) g_add_edge(g, sh, id - 1, id, layer_weight(qual, k - 1) + layer_weight(qual, k));
-        if (tail == -1) tail = id;
+        if (tail == -1) tail = tail_first = id;
+        ++tail_count;
     }
+    int cur_slot = kPendingSlot, first_start = -1;
     int prev_w = head == -1 ? 0 : layer_weight(qual, first_pos - 1);
     for (int k = naln - 1; k >= 0; --k) {
         const int pos = g.aln_pos[k];
@@ -400,8 +452,13 @@ __device__ void g_add_alignment(const Graph& g, PoaShared& sh, const uint8_t* se
         int nid;
         if (at == -1) {
             nid = g_add_node(g, sh, letter);
+            if (nid < 0) return;
+            g.nw_node[nnew] = nid;
+            g.nw_slot[nnew++] = cur_slot;
         } else if (g.code[at] == letter) {
             nid = at;
+            cur_slot = group_end_rank(g, at, nold);
+            if (first_start == -1) first_start = group_start_rank(g, at, nold);
         } else {
             int hit = -1;
             for (int x = g.al_head[at]; x != -1; x = g.a_next[x]) {
@@ -410,6 +467,8 @@ __device__ void g_add_alignment(const Graph& g, PoaShared& sh, const uint8_t* se
                     break;
                 }
             }
+            cur_slot = group_end_rank(g, at, nold);
+            if (first_start == -1) first_start = group_start_rank(g, at, nold);
             if (hit == -1) {
                 nid = g_add_node(g, sh, letter);
                 if (nid < 0) return;
@@ -420,19 +479,62 @@ __device__ void g_add_alignment(const Graph& g, PoaShared& sh, const uint8_t* se
                 }
                 g_add_aligned(g, sh, nid, at);
                 g_add_aligned(g, sh, at, nid);
+                g.nw_node[nnew] = nid;
+                g.nw_slot[nnew++] = cur_slot;
             } else {
                 nid = hit;
             }
         }
         if (nid < 0 || sh.fail) return;
         if (count_cov) g.cov[nid] += 1;
-        if (begin_id == -1) begin_id = nid;
         if (head != -1) g_add_edge(g, sh, head, nid, prev_w + layer_weight(qual, pos));
         head = nid;
         prev_w = layer_weight(qual, pos);
     }
     if (tail != -1) g_add_edge(g, sh, head, tail, prev_w + layer_weight(qual, last_pos + 1));
+    for (int t = 0; t < tail_count; ++t) {
+        g.nw_node[nnew] = tail_first + t;
+        g.nw_slot[nnew++] = cur_slot;
+    }
+    const int before = first_start == -1 ? nold - 1 : first_start - 1;
+    for (int t = 0; t < nnew; ++t)
+        if (g.nw_slot[t] == kPendingSlot) g.nw_slot[t] = before;
+    sh.nnew = nnew;
     sh.nseq += 1;
+}
+
+// Splices the new nodes of the last insertion into the incremental order
+// (warp): an old node at rank r moves up by the number of new nodes with slot
+// < r, the k-th new node (slots sorted) lands at slot + 1 + k.
+__device__ void order_insert(const Graph& g, const PoaShared& sh, int nold, int lane) {
+    const int nnew = sh.nnew, n = nold + nnew;
+    for (int r = lane; r <= nold; r += 32) g.shift[r] = 0;
+    __syncwarp();
+    for (int k = lane; k < nnew; k += 32) {
+        const int at = g.nw_slot[k] + 1;
+        if (at < nold) atomicAdd(&g.shift[at], 1);
+    }
+    __syncwarp();
+    int base = 0;
+    for (int c0 = 0; c0 < nold; c0 += 32) {
+        const int r = c0 + lane;
+        int v = r < nold ? g.shift[r] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        if (r < nold) g.ord2[r + base + v] = g.ord[r];
+        base += __shfl_sync(0xffffffffu, v, 31);
+    }
+    for (int k = lane; k < nnew; k += 32) g.ord2[g.nw_slot[k] + 1 + k] = g.nw_node[k];
+    __syncwarp();
+    for (int x = lane; x < n; x += 32) {
+        const int v = g.ord2[x];
+        g.ord[x] = v;
+        g.my_rank[v] = x;
+    }
+    __syncwarp();
 }
 
 __device__ int g_branch_completion(const Graph& g, PoaShared& sh, int rank) {
@@ -511,70 +613,482 @@ __device__ int g_heaviest_bundle(const Graph& g, PoaShared& sh) {
     return len;
 }
 
-// ---------------- block helpers ----------------
+// ---------------- DP of one layer (one warp) ----------------
 
-// Inclusive block scan of max-plus segments: element = (value at segment
-// end, segment length). Returns the exclusive carry (value at the position
-// before this thread's segment, kNegInf for the first).
-__device__ int block_carry_scan(PoaShared& sh, int v, int len, int gap) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    // inclusive warp scan
-    int sv = v, sl = len;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int pv = __shfl_up_sync(0xffffffffu, sv, o);
-        const int pl = __shfl_up_sync(0xffffffffu, sl, o);
-        if (lane >= o) {
-            const int cand = pv <= kNegInf / 2 ? kNegInf : pv + sl * gap;
-            sv = max(sv, cand);
-            sl = pl + sl;
-        }
-    }
-    if (lane == 31) {
-        sh.scan_v[wid] = sv;
-        sh.scan_l[wid] = sl;
-    }
-    __syncthreads();
-    // carry from previous warps
-    int cv = kNegInf;
-    for (int w = 0; w < wid; ++w) {
-        const int wv = sh.scan_v[w], wl = sh.scan_l[w];
-        cv = max(wv, cv <= kNegInf / 2 ? kNegInf : cv + wl * gap);
-    }
-    // inclusive value of this thread with warp-carry applied
-    int incl = max(sv, cv <= kNegInf / 2 ? kNegInf : cv + sl * gap);
-    // exclusive: shift by one lane
-    int excl = __shfl_up_sync(0xffffffffu, incl, 1);
-    if (lane == 0) excl = cv;
-    __syncthreads();
-    return excl;
+// Columns covered by one warp pass: S cells per lane, S a multiple of 4.
+__host__ __device__ inline int seg_cells(int wc) {
+    const int s = (wc + 31) / 32;
+    return s <= 24 ? ((s + 3) & ~3) : 24;
+}
+__host__ __device__ inline int row_cover(int wc) {
+    const int s = seg_cells(wc);
+    const int ch = 32 * s;
+    return ((wc + ch - 1) / ch) * ch;
 }
 
-// ---------------- one window ----------------
+constexpr uint32_t kNoPred = 0xFFu;
+constexpr uint32_t kEscape = 63u;  // predecessor index >= 63: decide again in the walk
 
-__device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint32_t wi, int* s_seq_row) {
-    const int tid = threadIdx.x;
+// DP of one layer against rows order[0..ndp) (ranks 1..ndp; rank 0 = empty
+// prefix row). Lane l owns columns [c + l*S, c + l*S + S) of each chunk c of
+// 32*S columns. Per cell it keeps T = max over predecessors of the diagonal
+// and vertical terms, the first predecessor giving T diagonally and the first
+// giving it vertically; the horizontal term is a max-plus scan: in-lane
+// prefix, then a warp shuffle scan of lane aggregates. Decision byte: p
+// (diagonal via predecessor p), 64 + p (vertical), 128 (horizontal), 255
+// (predecessor index >= 63). Returns the rank of the NW end cell (first sink
+// in rank order with the best last-column value).
+template <int S>
+__device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, int ndp, const uint8_t* seq, int L,
+                        int lane) {
+    static_assert(S % 4 == 0 && S >= 4 && S <= 32, "segment");
+    constexpr unsigned kFull = 0xffffffffu;
+    const int lc = g.lcap;
+    int* const Hm = g.H;
+    uint8_t* const Dm = g.dec;
+    const int* const pred_off = g.pred_off;
+    const int* const pred_idx = g.pred_idx;
+    const uint8_t* const sinkf = g.sink;
+    const uint8_t* const codes = g.code;
+    const int wc = L + 1;
+    const int ch = 32 * S;
+    const int nch = (wc + ch - 1) / ch;
+    const int gap = a.gap, mt = a.match, mm = a.mismatch;
+    // virtual row 0: j * gap
+    for (int j = lane; j < nch * ch; j += 32) Hm[j] = j * gap;
+    __syncwarp();
+    const int lane_l = (L % ch) / S, k_l = L % S, ch_l = L / ch;
+    int best_v = kNegInf, best_r = INT_MAX, ties = 0;
+    for (int i = 1; i <= ndp; ++i) {
+        const int v = order[i - 1];
+        const uint32_t cmask = uint32_t(codes[v]) * 0x01010101u;
+        const int pb = pred_off[i - 1], pe = pred_off[i];
+        const int np = pe - pb;
+        const int cnt = np == 0 ? 1 : np;
+        const bool is_sink = sinkf[i - 1] != 0;
+        int carry_in = kNegInf;  // final H of the last column of the previous chunk
+        for (int c = 0; c < nch; ++c) {
+            const int j0 = c * ch + lane * S;
+            // sequence chars of columns j0 .. j0+S-1 (column j compares seq[j-1])
+            uint32_t eq[S / 4];
+#pragma unroll
+            for (int q = 0; q < S / 4; ++q) {
+                uint32_t w = 0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int j = j0 + 4 * q + b;
+                    const uint32_t ch8 = (j >= 1 && j <= L) ? uint32_t(seq[j - 1]) : 0u;
+                    w |= ch8 << (8 * b);
+                }
+                eq[q] = __vcmpeq4(w, cmask);
+            }
+            int T[S];
+            uint32_t code[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                T[k] = kNegInf;
+                code[k] = 0xFFFFu;
+            }
+            for (int p = 0; p < cnt; ++p) {
+                const int r = np == 0 ? 0 : pred_idx[pb + p];
+                const int4* hp4 = reinterpret_cast<const int4*>(Hm + r * lc + j0);
+                int hv[S];
+#pragma unroll
+                for (int q = 0; q < S / 4; ++q) {
+                    const int4 t4 = hp4[q];
+                    hv[4 * q] = t4.x;
+                    hv[4 * q + 1] = t4.y;
+                    hv[4 * q + 2] = t4.z;
+                    hv[4 * q + 3] = t4.w;
+                }
+                int left = __shfl_up_sync(kFull, hv[S - 1], 1);
+                if (lane == 0) left = j0 > 0 ? Hm[r * lc + j0 - 1] : kNegInf;
+                const uint32_t pc = p < int(kEscape) ? uint32_t(p) : kEscape;
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    const int prev = k == 0 ? left : hv[k - 1];
+                    const bool same = (eq[k / 4] >> (8 * (k % 4))) & 1u;
+                    const int dg = prev <= kNegInf / 2 ? kNegInf : prev + (same ? mt : mm);
+                    const int vt = hv[k] + gap;
+                    const int mx = max(dg, vt);
+                    if (mx > T[k]) {
+                        T[k] = mx;
+                        code[k] = (dg == mx ? pc : kNoPred) | ((vt == mx ? pc : kNoPred) << 8);
+                    } else if (mx == T[k]) {
+                        if ((code[k] & 0xFFu) == kNoPred && dg == mx) code[k] = (code[k] & 0xFF00u) | pc;
+                        if ((code[k] >> 8) == kNoPred && vt == mx) code[k] = (code[k] & 0xFFu) | (pc << 8);
+                    }
+                }
+            }
+            // horizontal term: in-lane prefix, warp scan of lane aggregates
+            int hk[S];
+            int run = kNegInf;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                run = max(T[k], run <= kNegInf / 2 ? kNegInf : run + gap);
+                hk[k] = run;
+            }
+            int x = run;
+            if (lane == 0 && carry_in > kNegInf / 2) x = max(x, carry_in + S * gap);
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFull, x, o);
+                if (lane >= o && y > kNegInf / 2) x = max(x, y + o * S * gap);
+            }
+            int carry = __shfl_up_sync(kFull, x, 1);
+            if (lane == 0) carry = carry_in;
+            int hrow[S];
+            uint32_t dec4[S / 4];
+#pragma unroll
+            for (int q = 0; q < S / 4; ++q) dec4[q] = 0;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int cin = carry <= kNegInf / 2 ? kNegInf : carry + (k + 1) * gap;
+                const int h = max(hk[k], cin);
+                hrow[k] = h;
+                uint32_t d;
+                if (h > T[k]) {
+                    d = 128u;
+                } else if ((code[k] & 0xFFu) != kNoPred) {
+                    d = code[k] & 0xFFu;
+                    if (d == kEscape) d = 255u;
+                } else {
+                    d = (code[k] >> 8);
+                    d = d == kEscape ? 255u : 64u + d;
+                }
+                dec4[k / 4] |= d << (8 * (k % 4));
+            }
+            int4* out4 = reinterpret_cast<int4*>(Hm + i * lc + j0);
+#pragma unroll
+            for (int q = 0; q < S / 4; ++q)
+                out4[q] = make_int4(hrow[4 * q], hrow[4 * q + 1], hrow[4 * q + 2], hrow[4 * q + 3]);
+            uint32_t* d4 = reinterpret_cast<uint32_t*>(Dm + size_t(i) * lc + j0);
+#pragma unroll
+            for (int q = 0; q < S / 4; ++q) d4[q] = dec4[q];
+            if (c == ch_l && lane == lane_l && is_sink) {
+                int val = kNegInf;
+#pragma unroll
+                for (int k = 0; k < S; ++k)
+                    if (k == k_l) val = hrow[k];
+                if (val > best_v) {
+                    best_v = val;
+                    best_r = i;
+                    ties = 1;
+                } else if (val == best_v) {
+                    ++ties;
+                }
+            }
+            carry_in = __shfl_sync(kFull, hrow[S - 1], 31);
+        }
+        __syncwarp();
+    }
+    // the owner lane of column L holds the end cell
+    return EndCell{__shfl_sync(kFull, best_r, lane_l), __shfl_sync(kFull, best_v, lane_l),
+                   __shfl_sync(kFull, ties, lane_l)};
+}
+
+constexpr int kRingBytesPerWarp = 16384;
+// last 512 bytes of each warp's ring hold the 32-row descriptor block
+constexpr int kRingDescOffset = (kRingBytesPerWarp - 512) / 16;
+
+// Single-pass form of dp_layer for rows of at most 32*S columns. A lane only
+// ever reads its own column segment of earlier rows (the left neighbour
+// comes by shuffle), so rows are served without any cross-lane memory
+// ordering: the last R rows sit in a shared-memory ring laid out
+// [row][S/4][lane] (conflict-free int4), older rows come from global memory.
+// The next row's metadata (node, code, predecessor range, first predecessor,
+// sink flag) is loaded one row ahead. Per cell the pass keeps only T (best
+// diagonal/vertical value) and two packed decision bytes; the final values
+// are h_k = max(T_k, h_{k-1} + g) from the warp-scanned carry, and the cell
+// is horizontal exactly when h_{k-1} + g > T_k.
+template <int S>
+__device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* order, int ndp, const uint8_t* seq, int L,
+                             int lane, int4* ring) {
+    static_assert(S % 4 == 0 && S >= 4 && S <= 24, "segment");
+    constexpr unsigned kFull = 0xffffffffu;
+    constexpr int Q = S / 4;
+    constexpr int R = (kRingBytesPerWarp - 512) / (S * 128);
+    static_assert(R >= 2, "ring");
+    const int lc = g.lcap;
+    int* const Hm = g.H;
+    uint8_t* const Dm = g.dec;
+    const int* const pred_idx = g.pred_idx;
+    const int gap = a.gap, mt = a.match, mm = a.mismatch;
+    const int j0 = lane * S;
+    uint32_t sc[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        uint32_t w = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int j = j0 + 4 * q + b;
+            w |= ((j >= 1 && j <= L) ? uint32_t(seq[j - 1]) : 0u) << (8 * b);
+        }
+        sc[q] = w;
+    }
+    // row 0 (empty graph prefix) in global memory for the traceback
+#pragma unroll
+    for (int k = 0; k < S; ++k) Hm[j0 + k] = (j0 + k) * gap;
+    const int lane_l = L / S, k_l = L % S;
+    int best_v = kNegInf, best_r = INT_MAX, ties = 0;
+    // row descriptors: one coalesced load per 32 rows, one block ahead,
+    // served from a 32-entry shared block
+    int4* const dblk = ring + kRingDescOffset;
+    const int4* const rowdesc = g.rowdesc;
+    int4 pre = lane < ndp ? rowdesc[lane] : make_int4(0, 0, 0, 0);
+    for (int i = 1; i <= ndp; ++i) {
+        const int bi = (i - 1) & 31;
+        if (bi == 0) {
+            __syncwarp();
+            dblk[lane] = pre;
+            __syncwarp();
+            const int nx = i - 1 + 32 + lane;
+            pre = nx < ndp ? rowdesc[nx] : make_int4(0, 0, 0, 0);
+        }
+        const int4 d = dblk[bi];
+        const int np = d.w & 0xFF;
+        const bool is_sink = (d.w >> 8) & 1;
+        const uint32_t cmask = uint32_t((d.w >> 16) & 0xFF) * 0x01010101u;
+        const int p0 = np > 3 ? pred_idx[d.x] : d.x;
+        uint32_t eq[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) eq[q] = __vcmpeq4(sc[q], cmask);
+        int T[S];
+        int hv[S];
+        // bit k: the diagonal through predecessor 0 gives T_k (spoa tests it first)
+        uint32_t dbit = 0;
+        auto load_row = [&](int r) {
+            if (r == 0) {
+#pragma unroll
+                for (int k = 0; k < S; ++k) hv[k] = (j0 + k) * gap;
+            } else {
+                const bool in_ring = i - r <= R;
+                const int4* src = in_ring ? ring + (r % R) * Q * 32 + lane
+                                          : reinterpret_cast<const int4*>(Hm + r * lc + j0);
+                const int stride = in_ring ? 32 : 1;
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const int4 t4 = src[q * stride];
+                    hv[4 * q] = t4.x;
+                    hv[4 * q + 1] = t4.y;
+                    hv[4 * q + 2] = t4.z;
+                    hv[4 * q + 3] = t4.w;
+                }
+            }
+        };
+        load_row(np == 0 ? 0 : p0);
+        {
+            int left = __shfl_up_sync(kFull, hv[S - 1], 1);
+            if (lane == 0) left = kNegInf;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int pv = k == 0 ? left : hv[k - 1];
+                const bool same = (eq[k / 4] >> (8 * (k % 4))) & 1u;
+                const int dg = pv + (same ? mt : mm);
+                const int vt = hv[k] + gap;
+                T[k] = max(dg, vt);
+                dbit |= uint32_t(dg >= vt) << k;
+            }
+        }
+        uint32_t vbit = ~0u;  // single predecessor: non-diagonal cells are vertical through it
+        for (int p = 1; p < np; ++p) {
+            load_row(np > 3 ? pred_idx[d.x + p] : (p == 1 ? d.y : d.z));
+            int left = __shfl_up_sync(kFull, hv[S - 1], 1);
+            if (lane == 0) left = kNegInf;
+            vbit = 0u;  // several predecessors: the walk decides the rest from H
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int pv = k == 0 ? left : hv[k - 1];
+                const bool same = (eq[k / 4] >> (8 * (k % 4))) & 1u;
+                const int mx = max(pv + (same ? mt : mm), hv[k] + gap);
+                dbit &= ~(uint32_t(mx > T[k]) << k);
+                T[k] = max(T[k], mx);
+            }
+        }
+        // horizontal term: in-lane prefix as 4 independent sub-chains, warp
+        // scan of the lane aggregates, then every cell from its sub-chain's
+        // carry-in
+        constexpr int C = S / 4;  // cells per sub-chain
+        int agg[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            int run = kNegInf;
+#pragma unroll
+            for (int k = c * C; k < (c + 1) * C; ++k) {
+                run = max(T[k], run + gap);
+                hv[k] = run;
+            }
+            agg[c] = run;
+        }
+        int x = agg[0];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) x = max(agg[c], x + C * gap);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x = max(x, y + o * S * gap);
+        }
+        int cin = __shfl_up_sync(kFull, x, 1);  // final value left of the segment
+        if (lane == 0) cin = kNegInf;
+        const int carry = cin;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int next = max(agg[c], cin + C * gap);
+#pragma unroll
+            for (int k = c * C; k < (c + 1) * C; ++k) hv[k] = max(hv[k], cin + (k - c * C + 1) * gap);
+            cin = next;
+        }
+        uint32_t dec4[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) dec4[q] = 0;
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            const int hl = (k == 0 ? carry : hv[k - 1]) + gap;
+            uint32_t dd;
+            if (hl > T[k]) {
+                dd = 128u;
+            } else if ((dbit >> k) & 1u) {
+                dd = 0u;
+            } else {
+                dd = (vbit >> k) & 1u ? 64u : 255u;
+            }
+            dec4[k / 4] |= dd << (8 * (k % 4));
+        }
+        int4* dst_g = reinterpret_cast<int4*>(Hm + i * lc + j0);
+        int4* dst_r = ring + (i % R) * Q * 32 + lane;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int4 v4 = make_int4(hv[4 * q], hv[4 * q + 1], hv[4 * q + 2], hv[4 * q + 3]);
+            dst_g[q] = v4;
+            dst_r[q * 32] = v4;
+        }
+        uint32_t* d4 = reinterpret_cast<uint32_t*>(Dm + size_t(i) * lc + j0);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d4[q] = dec4[q];
+        if (lane == lane_l && is_sink) {
+            int val = kNegInf;
+#pragma unroll
+            for (int k = 0; k < S; ++k)
+                if (k == k_l) val = hv[k];
+            if (val > best_v) {
+                best_v = val;
+                best_r = i;
+                ties = 1;
+            } else if (val == best_v) {
+                ++ties;
+            }
+        }
+    }
+    __syncwarp();
+    return EndCell{__shfl_sync(kFull, best_r, lane_l), __shfl_sync(kFull, best_v, lane_l),
+                   __shfl_sync(kFull, ties, lane_l)};
+}
+
+__device__ EndCell dp_dispatch(const PoaArgs& a, const Graph& g, const int* order, int ndp, const uint8_t* seq, int L,
+                           int lane, int4* ring) {
+    if (L + 1 <= 32 * 24) {
+        switch (seg_cells(L + 1)) {
+            case 4: return dp_layer_fast<4>(a, g, order, ndp, seq, L, lane, ring);
+            case 8: return dp_layer_fast<8>(a, g, order, ndp, seq, L, lane, ring);
+            case 12: return dp_layer_fast<12>(a, g, order, ndp, seq, L, lane, ring);
+            case 16: return dp_layer_fast<16>(a, g, order, ndp, seq, L, lane, ring);
+            case 20: return dp_layer_fast<20>(a, g, order, ndp, seq, L, lane, ring);
+            default: return dp_layer_fast<24>(a, g, order, ndp, seq, L, lane, ring);
+        }
+    }
+    return dp_layer<24>(a, g, order, ndp, seq, L, lane);
+}
+
+// Walk back from (iend, L) over the decision bytes (lane 0). Writes the
+// alignment (node id or -1, position or -1), end of path first.
+__device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const int* order, const uint8_t* seq,
+                          int L, int iend) {
+    const int lc = g.lcap;
+    int i = iend, j = L, n = 0;
+    if (iend == INT_MAX || iend < 1) return false;
+    while (!(i == 0 && j == 0)) {
+        if (n >= g.alncap) return false;
+        if (i == 0) {
+            g.aln_node[n] = -1;
+            g.aln_pos[n] = j - 1;
+            ++n;
+            --j;
+            continue;
+        }
+        uint32_t code = g.dec[size_t(i) * lc + j];
+        const int pb = g.pred_off[i - 1], np = g.pred_off[i] - pb;
+        const int v = order[i - 1];
+        if (code == 255u) {  // predecessor index >= 63: decide again from H
+            const int h = g.H[i * lc + j];
+            const int s = j > 0 ? (seq[j - 1] == g.code[v] ? a.match : a.mismatch) : 0;
+            const int cnt = np == 0 ? 1 : np;
+            code = 128u;
+            int pick = -1;
+            if (j > 0)
+                for (int p = 0; p < cnt && pick < 0; ++p) {
+                    const int r = np == 0 ? 0 : g.pred_idx[pb + p];
+                    if (g.H[r * lc + j - 1] + s == h) pick = p;
+                }
+            if (pick >= 0) {
+                code = 1000u + uint32_t(pick);
+            } else {
+                for (int p = 0; p < cnt && pick < 0; ++p) {
+                    const int r = np == 0 ? 0 : g.pred_idx[pb + p];
+                    if (g.H[r * lc + j] + a.gap == h) pick = p;
+                }
+                if (pick >= 0) code = 2000u + uint32_t(pick);
+            }
+        }
+        if (code < 64u || (code >= 1000u && code < 2000u)) {
+            const int p = code < 64u ? int(code) : int(code - 1000u);
+            g.aln_node[n] = v;
+            g.aln_pos[n] = j - 1;
+            ++n;
+            i = np == 0 ? 0 : g.pred_idx[pb + p];
+            --j;
+        } else if (code < 128u || code >= 2000u) {
+            const int p = code < 128u ? int(code - 64u) : int(code - 2000u);
+            g.aln_node[n] = v;
+            g.aln_pos[n] = -1;
+            ++n;
+            i = np == 0 ? 0 : g.pred_idx[pb + p];
+        } else {
+            if (j == 0) return false;
+            g.aln_node[n] = -1;
+            g.aln_pos[n] = j - 1;
+            ++n;
+            --j;
+        }
+    }
+    sh.naln = n;
+    return true;
+}
+
+// ---------------- one window (one warp) ----------------
+
+__device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint32_t wi, int lane, int4* ring) {
     const PoaWinDev W = a.wins[wi];
     const uint8_t* bb = a.in + W.bb_off;
     const uint8_t* bq = W.bq_off == kNoQual ? nullptr : a.in + W.bq_off;
     uint8_t* outp = reinterpret_cast<uint8_t*>(a.out) + W.out_off;
     const int B = int(W.bb_len);
     if (W.n_layers < 2) {
-        for (int i = tid; i < B; i += blockDim.x) outp[i] = bb[i];
-        if (tid == 0) {
+        for (int i = lane; i < B; i += 32) outp[i] = bb[i];
+        if (lane == 0) {
             a.out_len[wi] = uint32_t(B);
             a.flags[wi] = 0;
         }
         return;
     }
     if (B > g.ncap) {
-        if (tid == 0) {
+        if (lane == 0) {
             a.flags[wi] = kOverflow;
             a.out_len[wi] = 0;
         }
         return;
     }
     // backbone: chain of B nodes, edge weights from quality (0 with the dummy)
-    for (int i = tid; i < B; i += blockDim.x) {
+    for (int i = lane; i < B; i += 32) {
         g.code[i] = bb[i];
         g.cov[i] = B >= 2 ? 1u : 0u;
         g.al_head[i] = g.al_tail[i] = -1;
@@ -595,9 +1109,10 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         } else {
             g.out_head[i] = g.out_tail[i] = i;
         }
-        g.rank_to_node[i] = i;
+        g.ord[i] = i;
+        g.my_rank[i] = i;
     }
-    if (tid == 0) {
+    if (lane == 0) {
         sh.nnodes = B;
         sh.nedges = B - 1;
         sh.naligned = 0;
@@ -605,7 +1120,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         sh.nranks = B;
         sh.fail = 0;
     }
-    __syncthreads();
+    __syncwarp();
     unsigned long long cells = 0;
 
     for (uint32_t li = 0; li < W.n_layers; ++li) {
@@ -613,49 +1128,46 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         const uint8_t* seq = a.in + Lr.seq_off;
         const uint8_t* qual = Lr.qual_off == kNoQual ? nullptr : a.in + Lr.qual_off;
         const int L = int(Lr.len);
-        const int Wc = L + 1;
         const bool full = Lr.begin < W.offset && Lr.end > uint32_t(B) - W.offset;
-        // ---- choose the node set and its topological order ----
         const int N = sh.nnodes;
-        for (int i = tid; i < N; i += blockDim.x) {
+        for (int i = lane; i < N; i += 32) {
             g.member[i] = full ? 1 : 0;
-            g.mark[i] = 0;
-            g.prim[i] = 1;
             g.dprank[i] = 0;
         }
-        __syncthreads();
-        if (!full) {
-            if (tid == 0) {
-                if (!g_mark_subgraph(g, sh, int(Lr.begin), int(Lr.end))) sh.fail = kOverflow;
-                if (!sh.fail) {
-                    const int nr = g_topo_sort(g, sh, false, g.dporder);
-                    if (nr < 0) sh.fail = kOverflow;
-                    sh.ndp = nr;
-                }
-            }
-        } else if (tid == 0) {
-            sh.ndp = sh.nranks;
+        __syncwarp();
+        if (lane == 0) {
+            if (!full && !g_mark_subgraph(g, sh, int(Lr.begin), int(Lr.end))) sh.fail = kOverflow;
+            if (!sh.fail && row_cover(L + 1) > g.lcap) sh.fail = kOverflow;
         }
-        __syncthreads();
+        __syncwarp();
         if (sh.fail) break;
-        const int ndp = sh.ndp;
-        const int* order = full ? g.rank_to_node : g.dporder;
-        if (ndp + 1 > g.ncap + 1 || Wc > g.lcap) {
-            if (tid == 0) sh.fail = kOverflow;
-            __syncthreads();
-            break;
+        // DP rows: the incremental order, restricted to the subgraph for a
+        // partial layer (any topological order gives the same DP values)
+        int ndp = N;
+        const int* order = g.ord;
+        if (!full) {
+            int base = 0;
+            for (int c0 = 0; c0 < N; c0 += 32) {
+                const int r = c0 + lane;
+                const int v = r < N ? g.ord[r] : 0;
+                const bool in = r < N && g.member[v];
+                const unsigned m = __ballot_sync(0xffffffffu, in);
+                if (in) g.dporder[base + __popc(m & ((1u << lane) - 1u))] = v;
+                base += __popc(m);
+            }
+            ndp = base;
+            order = g.dporder;
+            __syncwarp();
         }
-        for (int i = tid; i < ndp; i += blockDim.x) g.dprank[order[i]] = i + 1;
-        // layer sequence into shared memory
-        for (int j = tid; j < L; j += blockDim.x) s_seq_row[j] = seq[j];
-        __syncthreads();
-        // ---- predecessor lists (DP ranks, in in-edge order) and sinks ----
-        for (int i = tid; i < ndp; i += blockDim.x) {
+        for (int i = lane; i < ndp; i += 32) g.dprank[order[i]] = i + 1;
+        __syncwarp();
+        // predecessor counts (DP ranks, in in-edge order) and sinks
+        for (int i = lane; i < ndp; i += 32) {
             const int v = order[i];
-            int cnt = 0;
+            int cntp = 0;
             for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e])
-                if (g.dprank[g.e_src[e]] > 0) ++cnt;
-            g.pred_off[i + 1] = cnt;
+                if (g.dprank[g.e_src[e]] > 0) ++cntp;
+            g.pred_off[i + 1] = cntp;
             bool sink = true;
             for (int e = g.out_head[v]; e != -1; e = g.e_next_out[e])
                 if (g.dprank[g.e_dst[e]] > 0) {
@@ -664,220 +1176,100 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
                 }
             g.sink[i] = sink ? 1 : 0;
         }
-        __syncthreads();
-        if (tid == 0) {
-            g.pred_off[0] = 0;
-            for (int i = 1; i <= ndp; ++i) g.pred_off[i] += g.pred_off[i - 1];
+        __syncwarp();
+        // exclusive prefix of the counts (warp scan over chunks of 32)
+        {
+            int base = 0;
+            for (int c0 = 0; c0 < ndp; c0 += 32) {
+                const int i = c0 + lane;
+                int vcount = i < ndp ? g.pred_off[i + 1] : 0;
+                int incl = vcount;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                if (i < ndp) g.pred_off[i + 1] = base + incl;
+                base += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) g.pred_off[0] = 0;
         }
-        __syncthreads();
-        for (int i = tid; i < ndp; i += blockDim.x) {
+        __syncwarp();
+        for (int i = lane; i < ndp; i += 32) {
             const int v = order[i];
             int k = g.pred_off[i];
+            const int k0 = k;
+            int pr[3] = {0, 0, 0};
             for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e]) {
                 const int r = g.dprank[g.e_src[e]];
-                if (r > 0) g.pred_idx[k++] = r;
+                if (r > 0) {
+                    if (k - k0 < 3) pr[k - k0] = r;
+                    g.pred_idx[k++] = r;
+                }
             }
+            // descriptor: x,y,z = first predecessor ranks (x = list offset when
+            // more than three), w = count | sink << 8 | base << 16
+            const int np = k - k0;
+            g.rowdesc[i] = make_int4(np > 3 ? k0 : pr[0], pr[1], pr[2],
+                                     np | (int(g.sink[i]) << 8) | (int(g.code[v]) << 16));
         }
-        // ---- DP ----
-        const int lc = g.lcap;
-        for (int j = tid; j < Wc; j += blockDim.x) g.H[j] = j * a.gap;
-        __syncthreads();
-        const int seg = (Wc + blockDim.x - 1) / blockDim.x;
-        const int j0 = min(Wc, tid * seg), j1 = min(Wc, j0 + seg);
-        int* sT = s_seq_row + L + 1;  // per-row temporaries, Wc entries
-        for (int i = 1; i <= ndp; ++i) {
-            const int v = order[i - 1];
-            const uint8_t cv = g.code[v];
-            const int pb = g.pred_off[i - 1], pe = g.pred_off[i];
-            const int np = pe - pb;
-            int* Hi = g.H + size_t(i) * lc;
-            // diagonal / vertical terms
-            for (int j = j0; j < j1; ++j) {
-                int t = kNegInf;
-                if (np == 0) {
-                    const int* Hp = g.H;
-                    t = Hp[j] + a.gap;
-                    if (j > 0) t = max(t, Hp[j - 1] + (s_seq_row[j - 1] == cv ? a.match : a.mismatch));
-                } else {
-                    for (int p = pb; p < pe; ++p) {
-                        const int* Hp = g.H + size_t(g.pred_idx[p]) * lc;
-                        t = max(t, Hp[j] + a.gap);
-                        if (j > 0) t = max(t, Hp[j - 1] + (s_seq_row[j - 1] == cv ? a.match : a.mismatch));
-                    }
-                }
-                sT[j] = t;
-            }
-            // segment prefix, then block carry
-            int run = kNegInf;
-            for (int j = j0; j < j1; ++j) {
-                run = max(sT[j], run <= kNegInf / 2 ? kNegInf : run + a.gap);
-                sT[j] = run;
-            }
-            const int carry = block_carry_scan(sh, run, j1 - j0, a.gap);
-            uint8_t* Di = g.dec + size_t(i) * lc;
-            for (int j = j0; j < j1; ++j) {
-                const int cin = carry <= kNegInf / 2 ? kNegInf : carry + (j - j0 + 1) * a.gap;
-                const int h = max(sT[j], cin);
-                Hi[j] = h;
-                // traceback decision in spoa's order
-                uint8_t code = 128;
-                const int s = j > 0 ? (s_seq_row[j - 1] == cv ? a.match : a.mismatch) : 0;
-                bool found = false;
-                const int cnt = np == 0 ? 1 : np;
-                if (j > 0) {
-                    for (int p = 0; p < cnt; ++p) {
-                        const int r = np == 0 ? 0 : g.pred_idx[pb + p];
-                        if (g.H[size_t(r) * lc + j - 1] + s == h) {
-                            code = p < 64 ? uint8_t(p) : uint8_t(255);
-                            found = true;
-                            break;
-                        }
-                    }
-                }
-                if (!found) {
-                    for (int p = 0; p < cnt; ++p) {
-                        const int r = np == 0 ? 0 : g.pred_idx[pb + p];
-                        if (g.H[size_t(r) * lc + j] + a.gap == h) {
-                            code = p < 64 ? uint8_t(64 + p) : uint8_t(255);
-                            found = true;
-                            break;
-                        }
-                    }
-                }
-                Di[j] = code;
-            }
-            __syncthreads();
-        }
+        __syncwarp();
+        const EndCell ec = dp_dispatch(a, g, order, ndp, seq, L, lane, ring);
         cells += (unsigned long long)ndp * (unsigned long long)L;
-        // ---- NW end: first sink in order with the best last-column score ----
-        int bv = kNegInf, br = INT_MAX;
-        for (int i = tid; i < ndp; i += blockDim.x) {
-            if (g.sink[i]) {
-                const int val = g.H[size_t(i + 1) * lc + L];
-                if (val > bv || (val == bv && i + 1 < br)) {
-                    bv = val;
-                    br = i + 1;
-                }
+        int iend = ec.row;
+        if (ec.ties > 1) {
+            // several sinks share the best last-column value: spoa takes the
+            // first in its own topological order of the aligned (sub)graph
+            for (int i = lane; i < N; i += 32) {
+                g.mark[i] = 0;
+                g.prim[i] = 1;
             }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const int ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            const int orr = __shfl_xor_sync(0xffffffffu, br, o);
-            if (ov > bv || (ov == bv && orr < br)) {
-                bv = ov;
-                br = orr;
-            }
-        }
-        if ((tid & 31) == 0) {
-            sh.red_v[tid >> 5] = bv;
-            sh.red_r[tid >> 5] = br;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            int vv = kNegInf, rr = INT_MAX;
-            for (int w = 0; w < int(blockDim.x >> 5); ++w) {
-                if (sh.red_v[w] > vv || (sh.red_v[w] == vv && sh.red_r[w] < rr)) {
-                    vv = sh.red_v[w];
-                    rr = sh.red_r[w];
-                }
-            }
-            sh.iend = rr;
-            // ---- traceback ----
-            int i = rr, j = L, n = 0;
-            bool bad = rr == INT_MAX;
-            while (!bad && !(i == 0 && j == 0)) {
-                if (n >= g.alncap) {
-                    bad = true;
-                    break;
-                }
-                if (i == 0) {
-                    g.aln_node[n] = -1;
-                    g.aln_pos[n] = j - 1;
-                    ++n;
-                    --j;
-                    continue;
-                }
-                uint8_t code = g.dec[size_t(i) * lc + j];
-                const int pb = g.pred_off[i - 1], np = g.pred_off[i] - pb;
-                const int v = order[i - 1];
-                if (code == 255) {  // predecessor index >= 64: decide again from H
-                    const int h = g.H[size_t(i) * lc + j];
-                    const int s = j > 0 ? (seq[j - 1] == g.code[v] ? a.match : a.mismatch) : 0;
-                    const int cnt = np == 0 ? 1 : np;
-                    code = 128;
-                    int pick = -1;
-                    if (j > 0)
-                        for (int p = 0; p < cnt && pick < 0; ++p) {
-                            const int r = np == 0 ? 0 : g.pred_idx[pb + p];
-                            if (g.H[size_t(r) * lc + j - 1] + s == h) pick = p;
-                        }
-                    if (pick >= 0) {
-                        const int r = np == 0 ? 0 : g.pred_idx[pb + pick];
-                        g.aln_node[n] = v;
-                        g.aln_pos[n] = j - 1;
-                        ++n;
-                        i = r;
-                        --j;
-                        continue;
-                    }
-                    for (int p = 0; p < cnt && pick < 0; ++p) {
-                        const int r = np == 0 ? 0 : g.pred_idx[pb + p];
-                        if (g.H[size_t(r) * lc + j] + a.gap == h) pick = p;
-                    }
-                    if (pick >= 0) {
-                        g.aln_node[n] = v;
-                        g.aln_pos[n] = -1;
-                        ++n;
-                        i = np == 0 ? 0 : g.pred_idx[pb + pick];
-                        continue;
-                    }
-                }
-                if (code < 64) {
-                    g.aln_node[n] = v;
-                    g.aln_pos[n] = j - 1;
-                    ++n;
-                    i = np == 0 ? 0 : g.pred_idx[pb + code];
-                    --j;
-                } else if (code < 128) {
-                    g.aln_node[n] = v;
-                    g.aln_pos[n] = -1;
-                    ++n;
-                    i = np == 0 ? 0 : g.pred_idx[pb + (code - 64)];
+            __syncwarp();
+            if (lane == 0) {
+                const int nr = g_topo_sort(g, sh, full, g.rank_to_node);
+                if (nr < 0) {
+                    sh.fail = kOverflow;
                 } else {
-                    if (j == 0) {
-                        bad = true;
-                        break;
+                    for (int r = 0; r < nr; ++r) g.node_rank[g.rank_to_node[r]] = r;
+                    int best = INT_MAX;
+                    for (int i = 1; i <= ndp; ++i) {
+                        if (!g.sink[i - 1] || g.H[i * g.lcap + L] != ec.value) continue;
+                        const int rr = g.node_rank[order[i - 1]];
+                        if (rr < best) {
+                            best = rr;
+                            iend = i;
+                        }
                     }
-                    g.aln_node[n] = -1;
-                    g.aln_pos[n] = j - 1;
-                    ++n;
-                    --j;
                 }
             }
-            sh.naln = n;
-            if (bad) sh.fail = kFailed;
-            // ---- insert the layer and re-sort ----
+            iend = __shfl_sync(0xffffffffu, iend, 0);
+        }
+        if (lane == 0) {
+            if (!sh.fail && !traceback(a, g, sh, order, seq, L, iend)) sh.fail = kFailed;
             if (!sh.fail) g_add_alignment(g, sh, seq, qual, L);
         }
-        __syncthreads();
+        __syncwarp();
         if (sh.fail) break;
+        order_insert(g, sh, N, lane);
+    }
+    // spoa's topological order of the final graph for the consensus
+    if (!sh.fail) {
         const int N2 = sh.nnodes;
-        for (int i = tid; i < N2; i += blockDim.x) {
+        for (int i = lane; i < N2; i += 32) {
             g.mark[i] = 0;
             g.prim[i] = 1;
         }
-        __syncthreads();
-        if (tid == 0) {
+        __syncwarp();
+        if (lane == 0) {
             const int nr = g_topo_sort(g, sh, true, g.rank_to_node);
             if (nr < 0) sh.fail = kOverflow;
             sh.nranks = nr;
         }
-        __syncthreads();
-        if (sh.fail) break;
+        __syncwarp();
     }
-    if (tid == 0 && cells) atomicAdd(a.cells, cells);
+    if (lane == 0 && cells) atomicAdd(a.cells, cells);
     if (sh.fail) {
-        if (tid == 0) {
+        if (lane == 0) {
             a.flags[wi] = uint8_t(sh.fail);
             a.out_len[wi] = 0;
         }
@@ -885,19 +1277,18 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
     }
     // ---- consensus ----
     const int N = sh.nnodes;
-    for (int i = tid; i < N; i += blockDim.x) {
+    for (int i = lane; i < N; i += 32) {
         g.bscore[i] = -1;
         g.bpred[i] = -1;
     }
-    __syncthreads();
-    if (tid == 0) {
+    __syncwarp();
+    if (lane == 0) {
         const int len = g_heaviest_bundle(g, sh);
         uint8_t flags = kPolished;
         if (len < 0) {
             flags = kFailed;
             a.out_len[wi] = 0;
         } else {
-            // per-node coverage = own + aligned nodes' coverage
             int b = 0, e = len - 1;
             if (W.tgs && a.trim) {
                 const uint32_t avg = W.n_layers / 2;
@@ -928,19 +1319,30 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         }
         a.flags[wi] = flags;
     }
+    __syncwarp();
 }
 
-__global__ void __launch_bounds__(kPoaThreads) poa_kernel(PoaArgs a) {
-    __shared__ PoaShared sh;
-    extern __shared__ int s_dyn[];
-    const Graph g = make_graph(a, blockIdx.x);
+constexpr int kWarpsPerCta = 4;
+
+__global__ void __launch_bounds__(32 * kWarpsPerCta, 3) poa_kernel(PoaArgs a) {
+    __shared__ PoaShared sh_all[kWarpsPerCta];
+    // the per-warp view of its scratch slot lives in shared memory so the
+    // ~35 array pointers are not held in registers across the DP
+    __shared__ Graph g_all[kWarpsPerCta];
+    extern __shared__ int4 ring_all[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int4* ring = ring_all + wid * (kRingBytesPerWarp / 16);
+    PoaShared& sh = sh_all[wid];
+    const uint32_t slot = blockIdx.x * kWarpsPerCta + wid;
+    if (lane == 0) g_all[wid] = make_graph(a, slot);
+    __syncwarp();
+    const Graph& g = g_all[wid];
     while (true) {
-        __syncthreads();
-        if (threadIdx.x == 0) sh.best_rank = int(atomicAdd(&a.counters[0], 1u));
-        __syncthreads();
-        const uint32_t k = uint32_t(sh.best_rank);
+        unsigned k = 0;
+        if (lane == 0) k = atomicAdd(&a.counters[0], 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
         if (k >= a.nwin) break;
-        poa_window(a, g, sh, a.order[k], s_dyn);
+        poa_window(a, g, sh, a.order[k], lane, ring);
     }
 }
 
@@ -1108,21 +1510,25 @@ void PoaEngine::run() {
     const uint32_t* h_order = h_order_.as<uint32_t>();
     for (size_t i = 0; i < n; ++i) todo[i] = h_order[i];
     int ncap = 4096;
-    while (uint32_t(ncap) < std::min<uint32_t>(max_nodes_cap_, 6144)) ncap *= 2;
     std::vector<uint8_t> flags(n);
     float total_ms = 0;
+    // DP row width: every layer's columns rounded up to whole warp passes
+    const uint32_t* lens_max = &max_len_;
+    const int lcap = row_cover(int(*lens_max) + 1);
     while (!todo.empty()) {
         const int ecap = 2 * ncap, acap = ncap;
-        const int lcap = int((max_len_ + 1 + 3) & ~3u);
         const size_t slot = walk_layout(ncap, ecap, acap, lcap, [](int, size_t) {});
-        const size_t budget = size_t(24) << 30;
-        size_t slots = std::min<size_t>(todo.size(), size_t(dev_.sm_count) * 4);
+        // resident windows (one warp each): enough to fill the SMs, bounded by
+        // a scratch budget
+        const size_t budget = size_t(48) << 30;
+        size_t slots = std::min<size_t>(todo.size(), size_t(dev_.sm_count) * 12);
         // RB_POA_SLOTS caps the resident windows (smaller scratch, e.g. for
         // profiler captures); results do not depend on it
-        if (const char* e = getenv("RB_POA_SLOTS")) slots = std::max<size_t>(1, std::min<size_t>(slots, strtoull(e, nullptr, 10)));
+        if (const char* e = getenv("RB_POA_SLOTS"))
+            slots = std::max<size_t>(1, std::min<size_t>(slots, strtoull(e, nullptr, 10)));
         while (slots > 1 && slots * slot > budget) slots /= 2;
+        slots = (slots + kWarpsPerCta - 1) / kWarpsPerCta * kWarpsPerCta;
         d_graph_.reserve(slots * slot);
-        d_order_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
         DevBuf& d_todo = d_dp_;
         d_todo.reserve(todo.size() * 4);
         check_cuda(cudaMemcpyAsync(d_todo.ptr, todo.data(), todo.size() * 4, cudaMemcpyHostToDevice, stream_),
@@ -1149,14 +1555,12 @@ void PoaEngine::run() {
         a.trim = trim_;
         a.counters = d_misc_.as<unsigned int>();
         a.cells = reinterpret_cast<unsigned long long*>(d_misc_.as<unsigned int>() + 8);
-        const size_t smem = size_t(2 * lcap + 8) * sizeof(int);
-        if (smem > 48 * 1024) {
-            check_cuda(cudaFuncSetAttribute(poa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-                       "cudaFuncSetAttribute");
-        }
         check_cuda(cudaMemsetAsync(d_misc_.ptr, 0, 64, stream_), "memset counters");
         check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
-        poa_kernel<<<int(slots), kPoaThreads, smem, stream_>>>(a);
+        const int smem = kWarpsPerCta * kRingBytesPerWarp;
+        check_cuda(cudaFuncSetAttribute(poa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                   "cudaFuncSetAttribute");
+        poa_kernel<<<int(slots / kWarpsPerCta), 32 * kWarpsPerCta, smem, stream_>>>(a);
         check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
         ++stats_.launches;
         unsigned long long cells = 0;
