@@ -240,58 +240,6 @@ struct PoaShared {
 
 // ---------------- graph primitives (thread 0) ----------------
 
-__device__ int g_add_node(const Graph& g, PoaShared& sh, uint8_t c) {
-    if (sh.nnodes >= g.ncap) {
-        sh.fail = kOverflow;
-        return -1;
-    }
-    const int id = sh.nnodes++;
-    g.code[id] = c;
-    g.cov[id] = 0;
-    g.in_head[id] = g.in_tail[id] = -1;
-    g.out_head[id] = g.out_tail[id] = -1;
-    g.al_head[id] = g.al_tail[id] = -1;
-    return id;
-}
-
-__device__ void g_add_edge(const Graph& g, PoaShared& sh, int b, int e, int w) {
-    for (int x = g.out_head[b]; x != -1; x = g.e_next_out[x]) {
-        if (g.e_dst[x] == e) {
-            g.e_w[x] += w;
-            return;
-        }
-    }
-    if (sh.nedges >= g.ecap) {
-        sh.fail = kOverflow;
-        return;
-    }
-    const int id = sh.nedges++;
-    g.e_src[id] = b;
-    g.e_dst[id] = e;
-    g.e_w[id] = w;
-    g.e_next_in[id] = -1;
-    g.e_next_out[id] = -1;
-    if (g.out_tail[b] == -1) g.out_head[b] = id;
-    else g.e_next_out[g.out_tail[b]] = id;
-    g.out_tail[b] = id;
-    if (g.in_tail[e] == -1) g.in_head[e] = id;
-    else g.e_next_in[g.in_tail[e]] = id;
-    g.in_tail[e] = id;
-}
-
-__device__ void g_add_aligned(const Graph& g, PoaShared& sh, int v, int x) {
-    if (sh.naligned >= g.acap) {
-        sh.fail = kOverflow;
-        return;
-    }
-    const int id = sh.naligned++;
-    g.a_node[id] = x;
-    g.a_next[id] = -1;
-    if (g.al_tail[v] == -1) g.al_head[v] = id;
-    else g.a_next[g.al_tail[v]] = id;
-    g.al_tail[v] = id;
-}
-
 // spoa's DFS topological order over the nodes with member flag set (all nodes
 // when all_nodes). Writes the order to out; returns its length, -1 on overflow.
 __device__ int g_topo_sort(const Graph& g, PoaShared& sh, bool all_nodes, int* out) {
@@ -394,113 +342,235 @@ __device__ int group_start_rank(const Graph& g, int v, int nold) {
     return r;
 }
 
-constexpr int kPendingSlot = INT_MIN;
-
-// Graph::add_alignment for one layer (alignment in g.aln_* reversed order,
-// entries [0, naln) from the end of the path back to its start). Also lists
-// the new nodes in path order with the rank slot of the old order after which
-// each one goes (g.nw_node / g.nw_slot, sh.nnew): head nodes before the
-// aligned group of the first existing node on the path, a node joining an
-// aligned group right after that group, every other new node after the
-// previous node on the path. The slots are non-decreasing along the path.
-__device__ void g_add_alignment(const Graph& g, PoaShared& sh, const uint8_t* seq, const uint8_t* qual,
-                                int len) {
-    sh.nnew = 0;
-    if (len == 0) return;
-    const int naln = sh.naln;
-    const int nold = sh.nnodes;
-    const bool count_cov = len >= 2;
-    int first_pos = -1, last_pos = -1;
-    for (int k = naln - 1; k >= 0; --k) {
-        if (g.aln_pos[k] != -1) {
-            if (first_pos == -1) first_pos = g.aln_pos[k];
-            last_pos = g.aln_pos[k];
-        }
+// Warp prefix helpers: exclusive prefix of v over lanes, and the total.
+__device__ __forceinline__ int warp_excl(int v, int lane, int& total) {
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
-    if (first_pos == -1) {  // no sequence position aligned: cannot happen for NW
-        sh.fail = kFailed;
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+// Graph::add_alignment for one layer, by the whole warp. A path visits every
+// node and every aligned group at most once, so the per-position work is
+// independent: classify each aligned base (existing node, new base, new
+// member of an aligned group), number the new nodes in spoa's order (head
+// bases, tail bases, then new aligned bases along the path), then in
+// parallel create nodes, aligned-group links, edges P[k-1] -> P[k] with
+// weight w[k-1] + w[k] (every sequence position k owns exactly one path node
+// P[k]) and coverage, and list the new nodes with their order slots (see
+// order_insert). Per-entry scratch lives in g.stack: [0,m) node, [m,2m) kind
+// | aligned-count << 2, [2m,3m) anchor slot, [3m,4m) group start.
+__device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t* seq, const uint8_t* qual,
+                                   int len, int lane) {
+    const int m = sh.naln;
+    const int nold = sh.nnodes;
+    if (len == 0) return;
+    if (m == 0 || 4 * m + 64 > g.scap) {
+        if (lane == 0) sh.fail = m == 0 ? kFailed : kOverflow;
+        __syncwarp();
         return;
     }
-    int nnew = 0;
-    // head part [0, first_pos), then tail part (last_pos, len)
-    int head = -1;
-    for (int k = 0; k < first_pos; ++k) {
-        const int id = g_add_node(g, sh, seq[k]);
-        if (id < 0) return;
-        if (count_cov) g.cov[id] += 1;
-        if (k > 0) g_add_edge(g, sh, id - 1, id, layer_weight(qual, k - 1) + layer_weight(qual, k));
-        head = id;
-        g.nw_node[nnew] = id;
-        g.nw_slot[nnew++] = kPendingSlot;
-    }
-    int tail = -1, tail_first = -1, tail_count = 0;
-    for (int k = last_pos + 1; k < len; ++k) {
-        const int id = g_add_node(g, sh, seq[k]);
-        if (id < 0) return;
-        if (count_cov) g.cov[id] += 1;
-        if (k > last_pos + 1) g_add_edge(g, sh, id - 1, id, layer_weight(qual, k - 1) + layer_weight(qual, k));
-        if (tail == -1) tail = tail_first = id;
-        ++tail_count;
-    }
-    int cur_slot = kPendingSlot, first_start = -1;
-    int prev_w = head == -1 ? 0 : layer_weight(qual, first_pos - 1);
-    for (int k = naln - 1; k >= 0; --k) {
-        const int pos = g.aln_pos[k];
-        if (pos == -1) continue;
-        const uint8_t letter = seq[pos];
+    int* e_nid = g.stack;
+    int* e_kind = g.stack + m;
+    int* e_slot = g.stack + 2 * m;
+    int* e_start = g.stack + 3 * m;
+    const int first_pos = g.aln_pos[m - 1], last_pos = g.aln_pos[0];
+    const int h = first_pos, tl = len - 1 - last_pos;
+    // 1. classify (reads only the graph as it was before this insertion)
+    for (int t = lane; t < m; t += 32) {
+        const int k = m - 1 - t;
         const int at = g.aln_node[k];
-        int nid;
-        if (at == -1) {
-            nid = g_add_node(g, sh, letter);
-            if (nid < 0) return;
-            g.nw_node[nnew] = nid;
-            g.nw_slot[nnew++] = cur_slot;
-        } else if (g.code[at] == letter) {
-            nid = at;
-            cur_slot = group_end_rank(g, at, nold);
-            if (first_start == -1) first_start = group_start_rank(g, at, nold);
-        } else {
-            int hit = -1;
-            for (int x = g.al_head[at]; x != -1; x = g.a_next[x]) {
-                if (g.code[g.a_node[x]] == letter) {
-                    hit = g.a_node[x];
-                    break;
-                }
-            }
-            cur_slot = group_end_rank(g, at, nold);
-            if (first_start == -1) first_start = group_start_rank(g, at, nold);
-            if (hit == -1) {
-                nid = g_add_node(g, sh, letter);
-                if (nid < 0) return;
-                for (int x = g.al_head[at]; x != -1; x = g.a_next[x]) {
-                    const int y = g.a_node[x];
-                    g_add_aligned(g, sh, nid, y);
-                    g_add_aligned(g, sh, y, nid);
-                }
-                g_add_aligned(g, sh, nid, at);
-                g_add_aligned(g, sh, at, nid);
-                g.nw_node[nnew] = nid;
-                g.nw_slot[nnew++] = cur_slot;
+        const uint8_t letter = seq[g.aln_pos[k]];
+        int kind = 1, nid = -1, nal = 0, slot = INT_MIN, start = INT_MAX;
+        if (at != -1) {
+            slot = group_end_rank(g, at, nold);
+            start = group_start_rank(g, at, nold);
+            if (g.code[at] == letter) {
+                kind = 0;
+                nid = at;
             } else {
-                nid = hit;
+                for (int x = g.al_head[at]; x != -1; x = g.a_next[x]) {
+                    ++nal;
+                    if (nid == -1 && g.code[g.a_node[x]] == letter) nid = g.a_node[x];
+                }
+                kind = nid == -1 ? 2 : 0;
             }
         }
-        if (nid < 0 || sh.fail) return;
-        if (count_cov) g.cov[nid] += 1;
-        if (head != -1) g_add_edge(g, sh, head, nid, prev_w + layer_weight(qual, pos));
-        head = nid;
-        prev_w = layer_weight(qual, pos);
+        e_nid[t] = nid;
+        e_kind[t] = kind | (kind == 2 ? nal << 2 : 0);
+        e_slot[t] = slot;
+        e_start[t] = start;
     }
-    if (tail != -1) g_add_edge(g, sh, head, tail, prev_w + layer_weight(qual, last_pos + 1));
-    for (int t = 0; t < tail_count; ++t) {
-        g.nw_node[nnew] = tail_first + t;
-        g.nw_slot[nnew++] = cur_slot;
+    __syncwarp();
+    // 2. ids of new aligned bases, aligned-pool offsets, order slots
+    const int base_id = nold + h + tl;
+    int nnew_e = 0, nal_tot = 0, cur_slot = INT_MIN, first_start = INT_MAX;
+    for (int c0 = 0; c0 < m; c0 += 32) {
+        const int t = c0 + lane;
+        const int kd = t < m ? e_kind[t] : 0;
+        const int kind = kd & 3;
+        const bool is_new = t < m && kind != 0;
+        int tot;
+        const int pre = warp_excl(is_new ? 1 : 0, lane, tot);
+        int atot;
+        const int apre = warp_excl(kind == 2 ? 2 * (kd >> 2) + 2 : 0, lane, atot);
+        // last anchor slot up to t (anchors: kind 0 or 2), carried over chunks
+        int sl = (t < m && kind != 1) ? e_slot[t] : INT_MIN;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, sl, o);
+            if (lane >= o) sl = max(sl, y);
+        }
+        sl = max(sl, cur_slot);
+        int st = (t < m && kind != 1) ? e_start[t] : INT_MAX;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) st = min(st, __shfl_xor_sync(0xffffffffu, st, o));
+        if (first_start == INT_MAX) first_start = st;
+        if (t < m) {
+            if (is_new) e_nid[t] = base_id + nnew_e + pre;
+            // kind 2: own group slot; kind 1: last anchor before it (INT_MIN: none yet)
+            e_slot[t] = kind == 2 ? e_slot[t] : sl;
+            e_start[t] = nal_tot + apre;  // aligned-pool offset (kind 2)
+        }
+        cur_slot = __shfl_sync(0xffffffffu, sl, 31);
+        nnew_e += tot;
+        nal_tot += atot;
     }
-    const int before = first_start == -1 ? nold - 1 : first_start - 1;
-    for (int t = 0; t < nnew; ++t)
-        if (g.nw_slot[t] == kPendingSlot) g.nw_slot[t] = before;
-    sh.nnew = nnew;
-    sh.nseq += 1;
+    const int nnew = h + tl + nnew_e;
+    if (nold + nnew > g.ncap || sh.nedges + len + 2 > g.ecap || sh.naligned + nal_tot > g.acap) {
+        if (lane == 0) sh.fail = kOverflow;
+        __syncwarp();
+        return;
+    }
+    __syncwarp();
+    // 3. new nodes
+    auto path_node = [&](int k) -> int {
+        if (k < first_pos) return nold + k;
+        if (k > last_pos) return nold + h + (k - last_pos - 1);
+        return e_nid[k - first_pos];
+    };
+    for (int x = lane; x < nnew; x += 32) {
+        int id, k;
+        if (x < h) {
+            id = nold + x;
+            k = x;
+        } else if (x < h + tl) {
+            id = nold + x;
+            k = last_pos + 1 + (x - h);
+        } else {
+            id = nold + x;
+            k = -1;
+        }
+        g.code[id] = k >= 0 ? seq[k] : 0;
+        g.cov[id] = 0;
+        g.in_head[id] = g.in_tail[id] = -1;
+        g.out_head[id] = g.out_tail[id] = -1;
+        g.al_head[id] = g.al_tail[id] = -1;
+    }
+    __syncwarp();
+    for (int t = lane; t < m; t += 32) {
+        if ((e_kind[t] & 3) != 0) g.code[e_nid[t]] = seq[first_pos + t];
+    }
+    __syncwarp();
+    // 4. aligned groups: a new base joining the group of `at` links to every
+    //    member, then to `at` (spoa's order)
+    for (int t = lane; t < m; t += 32) {
+        if ((e_kind[t] & 3) != 2) continue;
+        const int at = g.aln_node[m - 1 - t];
+        const int G = e_nid[t];
+        int slot = sh.naligned + e_start[t];
+        auto link = [&](int v, int y) {
+            g.a_node[slot] = y;
+            g.a_next[slot] = -1;
+            if (g.al_tail[v] == -1) g.al_head[v] = slot;
+            else g.a_next[g.al_tail[v]] = slot;
+            g.al_tail[v] = slot;
+            ++slot;
+        };
+        for (int x = g.al_head[at]; x != -1; x = g.a_next[x]) {
+            const int y = g.a_node[x];
+            link(G, y);
+            link(y, G);
+        }
+        link(G, at);
+        link(at, G);
+    }
+    __syncwarp();
+    // 5. edges P[k-1] -> P[k]: existing ones gain weight, new ones are appended
+    int new_edges = 0;
+    for (int c0 = 1; c0 < len; c0 += 32) {
+        const int k = c0 + lane;
+        int u = -1, v = -1, w = 0, found = -1;
+        if (k < len) {
+            u = path_node(k - 1);
+            v = path_node(k);
+            w = layer_weight(qual, k - 1) + layer_weight(qual, k);
+            if (u < nold)
+                for (int e = g.out_head[u]; e != -1; e = g.e_next_out[e])
+                    if (g.e_dst[e] == v) {
+                        found = e;
+                        break;
+                    }
+        }
+        int tot;
+        const int pre = warp_excl((k < len && found < 0) ? 1 : 0, lane, tot);
+        __syncwarp();
+        if (k < len) {
+            if (found >= 0) {
+                g.e_w[found] += w;
+            } else {
+                const int id = sh.nedges + new_edges + pre;
+                g.e_src[id] = u;
+                g.e_dst[id] = v;
+                g.e_w[id] = w;
+                g.e_next_in[id] = -1;
+                g.e_next_out[id] = -1;
+                if (g.out_tail[u] == -1) g.out_head[u] = id;
+                else g.e_next_out[g.out_tail[u]] = id;
+                g.out_tail[u] = id;
+                if (g.in_tail[v] == -1) g.in_head[v] = id;
+                else g.e_next_in[g.in_tail[v]] = id;
+                g.in_tail[v] = id;
+            }
+        }
+        new_edges += tot;
+        __syncwarp();
+    }
+    // 6. coverage: every node of a path with at least two bases
+    if (len >= 2)
+        for (int k = lane; k < len; k += 32) g.cov[path_node(k)] += 1;
+    // 7. new nodes with their order slots, in path order
+    const int before = first_start == INT_MAX ? nold - 1 : first_start - 1;
+    const int last_slot = cur_slot == INT_MIN ? before : cur_slot;
+    for (int x = lane; x < h; x += 32) {
+        g.nw_node[x] = nold + x;
+        g.nw_slot[x] = before;
+    }
+    for (int t = lane; t < m; t += 32) {
+        if ((e_kind[t] & 3) == 0) continue;
+        const int id = e_nid[t];
+        const int at = id - base_id;  // position among the new aligned bases
+        const int sl = e_slot[t];
+        g.nw_node[h + at] = id;
+        g.nw_slot[h + at] = sl == INT_MIN ? before : sl;
+    }
+    for (int x = lane; x < tl; x += 32) {
+        g.nw_node[h + nnew_e + x] = nold + h + x;
+        g.nw_slot[h + nnew_e + x] = last_slot;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        sh.nnodes = nold + nnew;
+        sh.nedges += new_edges;
+        sh.naligned += nal_tot;
+        sh.nnew = nnew;
+        sh.nseq += 1;
+    }
+    __syncwarp();
 }
 
 // Splices the new nodes of the last insertion into the incremental order
@@ -1000,7 +1070,9 @@ __device__ EndCell dp_dispatch(const PoaArgs& a, const Graph& g, const int* orde
 }
 
 // Walk back from (iend, L) over the decision bytes (lane 0). Writes the
-// alignment (node id or -1, position or -1), end of path first.
+// sequence-consuming steps of the alignment (node id or -1 for an inserted
+// base, sequence position), end of path first; vertical steps (a graph node
+// against a gap) consume no position and add nothing to the graph.
 __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const int* order, const uint8_t* seq,
                           int L, int iend) {
     const int lc = g.lcap;
@@ -1048,10 +1120,7 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             --j;
         } else if (code < 128u || code >= 2000u) {
             const int p = code < 128u ? int(code - 64u) : int(code - 2000u);
-            g.aln_node[n] = v;
-            g.aln_pos[n] = -1;
-            ++n;
-            i = np == 0 ? 0 : g.pred_idx[pb + p];
+            i = np == 0 ? 0 : g.pred_idx[pb + p];  // vertical: no sequence position
         } else {
             if (j == 0) return false;
             g.aln_node[n] = -1;
@@ -1244,11 +1313,10 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
             }
             iend = __shfl_sync(0xffffffffu, iend, 0);
         }
-        if (lane == 0) {
-            if (!sh.fail && !traceback(a, g, sh, order, seq, L, iend)) sh.fail = kFailed;
-            if (!sh.fail) g_add_alignment(g, sh, seq, qual, L);
-        }
+        if (lane == 0 && !sh.fail && !traceback(a, g, sh, order, seq, L, iend)) sh.fail = kFailed;
         __syncwarp();
+        if (sh.fail) break;
+        add_alignment_warp(g, sh, seq, qual, L, lane);
         if (sh.fail) break;
         order_insert(g, sh, N, lane);
     }
