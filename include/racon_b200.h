@@ -217,6 +217,30 @@ size_t rb_job_windows(const rb_job* job, const rb_window** windows);
 void rb_job_free(rb_job* job);
 void rb_free(void* p);
 
+/* Edit distance of one pair (edlib NW semantics, the same value as
+ * rb_align_batch's edit_distance) that allocates no memory. No counterpart in
+ * the reference: racon always aligns through edlibAlign, which allocates.
+ *
+ * For callers that cannot allocate at the time they align: code that must not
+ * synchronise the device (cudaMalloc and cudaFree can wait for all work on
+ * it), and code running under a fixed device-memory budget that has already
+ * been handed out (a failed allocation there would end the job). Scratch lives in one static device array of about
+ * 1.6 MB per device, so each sequence is limited to 131072 bytes; longer
+ * inputs return RB_ERR_ARG with that message. The pair must have at most 32
+ * distinct byte values, else *distance is set to -1.
+ *
+ * query, target and distance are DEVICE pointers; the kernel runs one warp on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and the call returns
+ * without waiting for it. The current device's first call does one-time set-up
+ * (loads the kernel, looks up the array's address) and should come before any
+ * stream capture. All calls on a device share the array: it keeps the last
+ * call's contents and nothing in it needs to start at zero, but calls whose
+ * kernels can overlap (different streams without ordering) race on it and
+ * give wrong results, so order them on one stream. `err` (optional, capacity
+ * err_capacity bytes) receives a message on failure; no context is used. */
+int rb_nw_distance_noalloc(const char* query, uint32_t query_length, const char* target, uint32_t target_length,
+                           int32_t* distance, void* stream, char* err, uint32_t err_capacity);
+
 #ifdef __cplusplus
 }
 #endif

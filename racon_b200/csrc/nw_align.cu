@@ -43,8 +43,10 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 
 #include "rb_internal.hpp"
@@ -814,6 +816,92 @@ __global__ void cigar_breakpoints_kernel(const char* cig, const CigarOvlDev* ov,
     bp_count[i] = cnt;
 }
 
+
+// ---------------------------------------------------------------------------
+// Allocation-free edit distance (rb_nw_distance_noalloc). Same banded block
+// sweep and k doubling as nw_distance_kernel, for one pair, with every byte of
+// scratch (symbol-coded sequences, the two strip carry buffers) in one
+// file-scope device array instead of cudaMalloc'd memory. Every call on a
+// device uses the same array: it keeps the last call's contents, nothing in it
+// has to start at zero (each call writes every byte it later reads), and two
+// calls whose kernels overlap in time race on it.
+constexpr uint32_t kNoAllocMaxLen = 1u << 17;  // per sequence
+constexpr size_t kNoAllocCarry = size_t(kNoAllocMaxLen) + 64;
+constexpr size_t kNoAllocScratchBytes =
+    2 * size_t(kNoAllocMaxLen) + 2 * kNoAllocCarry + 2 * 4 * kNoAllocCarry + 4096;
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+__global__ void __launch_bounds__(32) nw_distance_noalloc_kernel(const char* q, uint32_t m, const char* t,
+                                                                 uint32_t n, int32_t* out, uint8_t* scratch) {
+    __shared__ u64 peq[kMaxSym * 32];
+    __shared__ int present[256];
+    const int lane = threadIdx.x;
+    if (m == 0 || n == 0) {
+        if (lane == 0) *out = int32_t(max(m, n));
+        return;
+    }
+    uint8_t* qc = scratch;
+    uint8_t* tc = scratch + kNoAllocMaxLen;
+    WarpScratch ws;
+    uint8_t* p = scratch + 2 * size_t(kNoAllocMaxLen);
+    ws.carry_h[0] = reinterpret_cast<int8_t*>(p);
+    ws.carry_h[1] = reinterpret_cast<int8_t*>(p + kNoAllocCarry);
+    p += 2 * kNoAllocCarry;
+    p = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 255) & ~uintptr_t(255));
+    ws.carry_s[0] = reinterpret_cast<int32_t*>(p);
+    ws.carry_s[1] = reinterpret_cast<int32_t*>(p + 4 * kNoAllocCarry);
+    ws.capl_pv = ws.capl_mv = ws.capr_pv = ws.capr_mv = nullptr;
+    ws.capl_sc = ws.capr_sc = nullptr;
+    ws.leaf = nullptr;
+    // symbols present, numbered by byte value (the distance does not depend
+    // on the numbering); more than 32 distinct symbols is reported as -1
+    for (int c = lane; c < 256; c += 32) present[c] = 0;
+    __syncwarp();
+    for (uint32_t i = lane; i < m; i += 32) present[uint8_t(q[i])] = 1;
+    for (uint32_t i = lane; i < n; i += 32) present[uint8_t(t[i])] = 1;
+    __syncwarp();
+    int nsym = 0;
+    for (int c = 0; c < 256; ++c) nsym += present[c];
+    __syncwarp();
+    if (nsym > kMaxSym) {
+        if (lane == 0) *out = -1;
+        return;
+    }
+    // present[c] := code of c (exclusive prefix over byte values)
+    if (lane == 0) {
+        int acc = 0;
+        for (int c = 0; c < 256; ++c) {
+            const int pr = present[c];
+            present[c] = acc;
+            acc += pr;
+        }
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < m; i += 32) qc[i] = uint8_t(present[uint8_t(q[i])]);
+    for (uint32_t i = lane; i < n; i += 32) tc[i] = uint8_t(present[uint8_t(t[i])]);
+    __syncwarp();
+    SweepIO io;
+    io.q = qc;
+    io.t = tc;
+    io.rev = false;
+    io.ncols = int(n);
+    io.nsym = max(nsym, 1);
+    io.peq = peq;
+    io.cap_pv = io.cap_mv = nullptr;
+    io.cap_sc = nullptr;
+    io.leaf = nullptr;
+    io.bw = 0;
+    int k = max(64, abs(int(m) - int(n)));
+    int d;
+    while (true) {
+        const Band B = make_band(int(m), int(n), k);
+        d = warp_sweep<kDistance>(io, B, ws, lane, nullptr);
+        if (d <= k) break;
+        k *= 2;
+    }
+    if (lane == 0) *out = d;
+}
+
 }  // namespace
 
 NwEngine::NwEngine(const DeviceInfo& dev, cudaStream_t stream) : dev_(dev), stream_(stream) {
@@ -1173,3 +1261,70 @@ void NwEngine::fetch(rb_aln_result* out) {
 }
 
 }  // namespace rb
+
+// ---------------------------------------------------------------------------
+// rb_nw_distance_noalloc: C entry point of the allocation-free variant.
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+int noalloc_fail(char* err, uint32_t cap, int code, const char* fmt, ...) {
+    if (err && cap) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(err, cap, fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+}  // namespace
+
+extern "C" int rb_nw_distance_noalloc(const char* query, uint32_t query_length, const char* target,
+                                      uint32_t target_length, int32_t* distance, void* stream, char* err,
+                                      uint32_t err_capacity) {
+    if (err && err_capacity) err[0] = '\0';
+    if (!distance || (query_length && !query) || (target_length && !target))
+        return noalloc_fail(err, err_capacity, RB_ERR_ARG, "rb_nw_distance_noalloc: null pointer argument");
+    if (query_length > rb::kNoAllocMaxLen || target_length > rb::kNoAllocMaxLen)
+        return noalloc_fail(err, err_capacity, RB_ERR_ARG,
+                            "rb_nw_distance_noalloc: sequence length %llu exceeds the static scratch limit of %llu bytes",
+                            (unsigned long long)std::max(query_length, target_length),
+                            (unsigned long long)rb::kNoAllocMaxLen);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
+        return noalloc_fail(err, err_capacity, RB_ERR_CUDA, "rb_nw_distance_noalloc: no usable current device (CUDA error %d, device %d)",
+                            int(e), dev);
+    void* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            // One-time set-up on this device: load the kernel and look up the
+            // device address of the scratch array. Host code cannot take the
+            // address of a __device__ variable directly.
+            cudaFuncAttributes fa;
+            e = cudaFuncGetAttributes(&fa, rb::nw_distance_noalloc_kernel);
+            if (e != cudaSuccess)
+                return noalloc_fail(err, err_capacity, RB_ERR_CUDA,
+                                    "rb_nw_distance_noalloc: kernel load failed: %s", cudaGetErrorString(e));
+            void* ptr = nullptr;
+            e = cudaGetSymbolAddress(&ptr, rb::g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr)
+                return noalloc_fail(err, err_capacity, RB_ERR_CUDA,
+                                    "rb_nw_distance_noalloc: scratch address lookup failed: %s",
+                                    cudaGetErrorString(e));
+            g_noalloc_ptr[dev] = ptr;
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    rb::nw_distance_noalloc_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(
+        query, query_length, target, target_length, distance, static_cast<uint8_t*>(scratch));
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return noalloc_fail(err, err_capacity, RB_ERR_CUDA, "rb_nw_distance_noalloc: launch failed: %s",
+                            cudaGetErrorString(e));
+    return RB_OK;
+}
