@@ -227,6 +227,24 @@ def main():
     value = world * n_win * args.steps / dev_s_max
     gcups = cells / dev_s / 1e9
 
+    # ---- plain comparison form (one window per block, input order, no queue) ----
+    ctx.poa_run(plain=True)
+    plain_ms, plain_launches = [], 0
+    barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ctx.poa_run(plain=True)
+        st = ctx.poa_stats()
+        plain_ms.append(st.kernel_ms)
+        plain_launches += st.launches
+    barrier()
+    assert ctx.poa_fetch() == reference_out, "plain form results differ from the batched form"
+    t = torch.tensor([sum(plain_ms) / 1000.0], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    plain_value = world * n_win * args.steps / float(t.item())
+
     # ---- end to end through the C ABI with host buffers ----
     for _ in range(1):
         ctx.poa_job(job)
@@ -266,6 +284,11 @@ def main():
         "cells_per_step": cells // max(1, args.steps),
         "windows_per_step": n_win, "layers_per_step": n_layers,
         "gpu_launches": launches,
+        "plain": {"value": plain_value, "unit": "windows/s", "ms_per_step": sum(plain_ms) / max(1, args.steps),
+                  "launches_per_step": plain_launches // max(1, args.steps),
+                  "form": "one window per one-warp block, input order, one launch per batch, no queue; "
+                          "same per-window code, identical output (checked)"},
+        "batched_vs_plain": value / plain_value,
         "e2e": {"value": e2e_value, "unit": "windows/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
                 "d2h_bytes_per_step": d2h // max(1, args.steps)},
         "roofline": {"bound": "hbm", "kernel": "poa_kernel", "achieved": achieved_gbs,

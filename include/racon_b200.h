@@ -148,6 +148,12 @@ int rb_poa_stage(rb_ctx* ctx, const rb_window* windows, size_t n, int trim);
 int rb_poa_run(rb_ctx* ctx);
 int rb_poa_fetch(rb_ctx* ctx, rb_poa_result* out);
 
+/* Plain comparison form of rb_poa_run, for measurement only (no counterpart in
+ * the reference): the same per-window device code, but one window per
+ * one-warp block in input order, one launch per batch and no work queue.
+ * Results are identical to rb_poa_run's; fetch them with rb_poa_fetch. */
+int rb_poa_run_plain(rb_ctx* ctx);
+
 /* Breaking points of overlaps that already carry an alignment (SAM input:
  * src/overlap.cpp:192-200 skips the aligner when the CIGAR is set and walks
  * it in find_breaking_points_from_cigar, :226-292). cigar is the SAM CIGAR

@@ -109,6 +109,7 @@ def load():
                                  ctypes.POINTER(_PoaResult)]
     lib.rb_poa_stage.argtypes = [vp, ctypes.POINTER(_Window), ctypes.c_size_t, ctypes.c_int]
     lib.rb_poa_run.argtypes = [vp]
+    lib.rb_poa_run_plain.argtypes = [vp]
     lib.rb_poa_fetch.argtypes = [vp, ctypes.POINTER(_PoaResult)]
     lib.rb_poa_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.rb_align_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -267,8 +268,11 @@ class Context:
         self._check(self.lib.rb_poa_stage(self.ptr, arr, len(windows), int(trim)))
         self._staged_windows = len(windows)
 
-    def poa_run(self):
-        self._check(self.lib.rb_poa_run(self.ptr))
+    def poa_run(self, plain=False):
+        """Runs the staged windows: the batched form (size-sorted work queue),
+        or with plain=True the comparison form (one window per block, input
+        order, no queue). Both give identical results."""
+        self._check((self.lib.rb_poa_run_plain if plain else self.lib.rb_poa_run)(self.ptr))
 
     def poa_fetch(self):
         r = _PoaResult()

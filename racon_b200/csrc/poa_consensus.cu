@@ -1414,6 +1414,20 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, 3) poa_kernel(PoaArgs a) {
     }
 }
 
+// Plain comparison form: one window per one-warp block, block b takes window
+// order[b] with scratch slot b, one launch per batch, no work queue. Same
+// per-window code as poa_kernel, so results are identical.
+__global__ void __launch_bounds__(32 * kWarpsPerCta, 3) poa_plain_kernel(PoaArgs a) {
+    __shared__ PoaShared sh;
+    __shared__ Graph g;
+    extern __shared__ int4 ring_all[];
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x >= a.nwin) return;
+    if (lane == 0) g = make_graph(a, blockIdx.x);
+    __syncwarp();
+    poa_window(a, g, sh, a.order[blockIdx.x], lane, ring_all);
+}
+
 }  // namespace
 
 PoaEngine::PoaEngine(const DeviceInfo& dev, cudaStream_t stream, int8_t m, int8_t x, int8_t g)
@@ -1563,7 +1577,7 @@ void PoaEngine::stage(const rb_window* wins, size_t n, int trim) {
     in_bytes_ = off;
 }
 
-void PoaEngine::run() {
+void PoaEngine::run(bool plain) {
     const size_t n = nwin_;
     stats_.launches = 0;
     stats_.items = n;
@@ -1576,7 +1590,8 @@ void PoaEngine::run() {
     d_misc_.reserve(64);
     std::vector<uint32_t> todo(n);
     const uint32_t* h_order = h_order_.as<uint32_t>();
-    for (size_t i = 0; i < n; ++i) todo[i] = h_order[i];
+    // batched form: size-sorted queue; plain form: input order
+    for (size_t i = 0; i < n; ++i) todo[i] = plain ? uint32_t(i) : h_order[i];
     int ncap = 4096;
     std::vector<uint8_t> flags(n);
     float total_ms = 0;
@@ -1589,13 +1604,13 @@ void PoaEngine::run() {
         // resident windows (one warp each): enough to fill the SMs, bounded by
         // a scratch budget
         const size_t budget = size_t(48) << 30;
-        size_t slots = std::min<size_t>(todo.size(), size_t(dev_.sm_count) * 12);
+        size_t slots = std::min<size_t>(todo.size(), plain ? todo.size() : size_t(dev_.sm_count) * 12);
         // RB_POA_SLOTS caps the resident windows (smaller scratch, e.g. for
         // profiler captures); results do not depend on it
         if (const char* e = getenv("RB_POA_SLOTS"))
             slots = std::max<size_t>(1, std::min<size_t>(slots, strtoull(e, nullptr, 10)));
         while (slots > 1 && slots * slot > budget) slots /= 2;
-        slots = (slots + kWarpsPerCta - 1) / kWarpsPerCta * kWarpsPerCta;
+        if (!plain) slots = (slots + kWarpsPerCta - 1) / kWarpsPerCta * kWarpsPerCta;
         d_graph_.reserve(slots * slot);
         DevBuf& d_todo = d_dp_;
         d_todo.reserve(todo.size() * 4);
@@ -1625,12 +1640,26 @@ void PoaEngine::run() {
         a.cells = reinterpret_cast<unsigned long long*>(d_misc_.as<unsigned int>() + 8);
         check_cuda(cudaMemsetAsync(d_misc_.ptr, 0, 64, stream_), "memset counters");
         check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
-        const int smem = kWarpsPerCta * kRingBytesPerWarp;
-        check_cuda(cudaFuncSetAttribute(poa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-                   "cudaFuncSetAttribute");
-        poa_kernel<<<int(slots / kWarpsPerCta), 32 * kWarpsPerCta, smem, stream_>>>(a);
+        if (plain) {
+            // one launch per batch of `slots` windows
+            check_cuda(cudaFuncSetAttribute(poa_plain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            kRingBytesPerWarp),
+                       "cudaFuncSetAttribute");
+            for (size_t b0 = 0; b0 < todo.size(); b0 += slots) {
+                PoaArgs ab = a;
+                ab.order = a.order + b0;
+                ab.nwin = uint32_t(std::min(slots, todo.size() - b0));
+                poa_plain_kernel<<<int(ab.nwin), 32, kRingBytesPerWarp, stream_>>>(ab);
+                ++stats_.launches;
+            }
+        } else {
+            const int smem = kWarpsPerCta * kRingBytesPerWarp;
+            check_cuda(cudaFuncSetAttribute(poa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "cudaFuncSetAttribute");
+            poa_kernel<<<int(slots / kWarpsPerCta), 32 * kWarpsPerCta, smem, stream_>>>(a);
+            ++stats_.launches;
+        }
         check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
-        ++stats_.launches;
         unsigned long long cells = 0;
         check_cuda(cudaMemcpyAsync(&cells, a.cells, 8, cudaMemcpyDeviceToHost, stream_), "D2H cells");
         check_cuda(cudaMemcpyAsync(flags.data(), d_flags_.ptr, n, cudaMemcpyDeviceToHost, stream_), "D2H flags");

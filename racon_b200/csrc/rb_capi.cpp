@@ -180,6 +180,10 @@ int rb_poa_stage(rb_ctx* ctx, const rb_window* windows, size_t n, int trim) {
 int rb_poa_run(rb_ctx* ctx) {
     return guarded(ctx, [&]() { ctx->poa->run(); });
 }
+
+int rb_poa_run_plain(rb_ctx* ctx) {
+    return guarded(ctx, [&]() { ctx->poa->run(true); });
+}
 int rb_poa_fetch(rb_ctx* ctx, rb_poa_result* out) {
     if (!out) return RB_ERR_ARG;
     return guarded(ctx, [&]() { ctx->poa->fetch(out); });

@@ -97,7 +97,7 @@ public:
     PoaEngine(const DeviceInfo& dev, cudaStream_t stream, int8_t m, int8_t x, int8_t g);
     ~PoaEngine();
     void stage(const rb_window* wins, size_t n, int trim);
-    void run();
+    void run(bool plain = false);
     void fetch(rb_poa_result* out);
     const rb_stats& stats() const { return stats_; }
 

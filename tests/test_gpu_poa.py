@@ -72,3 +72,7 @@ def test_stage_run_fetch(native_lib, oracle_lib):
         ctx.poa_run()
         ctx.poa_run()
         assert ctx.poa_fetch() == a
+        # plain comparison form: same results
+        ctx.poa_run(plain=True)
+        assert ctx.poa_fetch() == a
+        assert ctx.poa_stats().launches >= 1
