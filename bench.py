@@ -34,6 +34,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+# DRAM bytes (read + write) per DP cell of poa_kernel, from one ncu capture of
+# config 1 at 0.1 genome scale (1.785 GB read + 30.877 GB written over
+# 5.839 G cells); traffic grows with the cells, so a full launch's traffic is
+# this times its cells
+POA_DRAM_BYTES_PER_CELL = (1.784984e9 + 30.877037e9) / 5838774640
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -293,7 +298,9 @@ def main():
                 "d2h_bytes_per_step": d2h // max(1, args.steps)},
         "roofline": {"bound": "hbm", "kernel": "poa_kernel", "achieved": achieved_gbs,
                      "peak": peaks.get("hbm_gbs", 6650.0), "unit": "GB/s",
-                     "frac": achieved_gbs / peaks.get("hbm_gbs", 6650.0), "traffic": None,
+                     "frac": achieved_gbs / peaks.get("hbm_gbs", 6650.0),
+                     "traffic": cells / max(1, launches) * POA_DRAM_BYTES_PER_CELL,
+                     "traffic_source": "ncu dram bytes of a 0.1-scale capture, scaled by DP cells per launch",
                      "peak_source": peak_kind,
                      "note": "algorithmic bytes = bases+qualities in + consensus out; the DP is integer-issue "
                              "bound, see compute"},
