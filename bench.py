@@ -48,11 +48,14 @@ def _args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--config", type=int, default=1, choices=[0, 1])
+    p.add_argument("--config", type=int, default=1, choices=[0, 1, 4])
     p.add_argument("--scale", type=float, default=1.0, help="genome scale (1.0 = the named workload)")
     p.add_argument("--cpu-sample", type=int, default=400, help="windows in the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--data-dir", default=None)
+    p.add_argument("--serving-jobs", type=int, default=12, help="config-4 jobs in the serving measurement "
+                   "(0 = skip it)")
+    p.add_argument("--workers", type=int, default=4, help="serving-loop workers")
     return p.parse_args()
 
 
@@ -150,11 +153,119 @@ def _cpu_baseline(job_windows, n_sample, match, mismatch, gap):
     return n, sec, cells, threads
 
 
+def _serving_jobs(args):
+    from racon_b200 import synthetic
+    base = args.data_dir or os.path.join(tempfile.gettempdir(), "racon_b200_bench")
+    d = os.path.join(base, "config4_n%d" % args.serving_jobs)
+    marker = os.path.join(d, "done.json")
+    if os.path.exists(marker):
+        with open(marker) as fh:
+            return json.load(fh)
+    jobs = synthetic.serving_jobs(d, args.serving_jobs, seed=4)
+    with open(marker, "w") as fh:
+        json.dump(jobs, fh)
+    return jobs
+
+
+def _pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q / 100.0 * (len(xs) - 1)))))
+    return xs[k]
+
+
+def run_serving(args, device, rates):
+    """Config 4: a stream of config-0-like jobs through the serving loop.
+    Isolated-job latency (each job alone on an idle server), peak throughput
+    (all jobs at once), then Poisson arrivals at fractions of that peak; every
+    output is checked against the job's isolated output."""
+    import random
+    import racon_b200
+    jobs = _serving_jobs(args)
+    w = 500
+    windows = [(j[3]["draft_length"] + w - 1) // w for j in jobs]
+    out = {"jobs": len(jobs), "workers": args.workers,
+           "job_shape": "contig log-uniform 20 kb-2 Mb, coverage U[20,80], error U[8,15]%, FASTA, PAF, "
+                        "-w 500 -m 3 -x -5 -g -4",
+           "windows": sum(windows)}
+    import torch
+    free_b, _ = torch.cuda.mem_get_info(device)
+    budget = int(free_b * 0.7)
+    out["hbm_budget"] = budget
+    with racon_b200.Server(device, workers=args.workers, hbm_budget=budget, match=3, mismatch=-5, gap=-4,
+                           window_length=w) as srv:
+        def run(arrivals):
+            t0 = time.perf_counter()
+            tickets = []
+            for i, j in enumerate(jobs):
+                if arrivals is not None:
+                    dt = arrivals[i] - (time.perf_counter() - t0)
+                    if dt > 0:
+                        time.sleep(dt)
+                tickets.append(srv.submit(j[0], j[1], j[2]))
+            res = [srv.wait(t) for t in tickets]
+            span = max(r[1]["finished"] for r in res) - min(r[1]["submitted"] for r in res)
+            return [r[0] for r in res], [r[1] for r in res], span
+
+        run(None)  # warm: every worker's device buffers reach their working size
+        iso, alone = [], []
+        for j in jobs:
+            fasta, tm = srv.wait(srv.submit(j[0], j[1], j[2]))
+            alone.append(fasta)
+            iso.append(tm["finished"] - tm["submitted"])
+        fastas, _, span = run(None)
+        assert fastas == alone, "a job's output differs between alone and in the mix"
+        peak = len(jobs) / span
+        out.update(isolated_s={"p50": _pct(iso, 50), "max": max(iso), "sum": sum(iso)},
+                   peak={"jobs_per_s": peak, "windows_per_s": sum(windows) / span, "makespan_s": span})
+        sweep = []
+        rng = random.Random(4)
+        for frac in rates:
+            lam = frac * peak
+            t, arrivals = 0.0, []
+            for _ in jobs:
+                arrivals.append(t)
+                t += rng.expovariate(lam)
+            fastas, times, span = run(arrivals)
+            assert fastas == alone, "a job's output differs between alone and in the mix"
+            lat = [tm["finished"] - tm["submitted"] for tm in times]
+            ratio = [a / b for a, b in zip(lat, iso)]
+            sweep.append({"load": frac, "jobs_per_s": len(jobs) / span, "windows_per_s": sum(windows) / span,
+                          "latency_s": {"p50": _pct(lat, 50), "p99": _pct(lat, 99)},
+                          "latency_vs_isolated": {"p50": _pct(ratio, 50), "p99": _pct(ratio, 99)}})
+        out["rates"] = sweep
+    return out
+
+
 def run_reference(args):
     world, rank, local = _dist()
     if rank != 0:
         return
     import oracle
+    if args.config == 4:
+        # the CPU oracle polishes the config-4 jobs one after another (a bounded sample of the stream)
+        jobs = _serving_jobs(args)
+        threads = os.cpu_count() or 1
+        done_w, total_s = 0, 0.0
+        for j in jobs:
+            t0 = time.perf_counter()
+            oracle.polish(j[0], j[1], j[2], threads=threads)
+            total_s += time.perf_counter() - t0
+            done_w += (j[3]["draft_length"] + 499) // 500
+            if total_s > 30:
+                break
+        value = done_w / total_s
+        print(json.dumps({"metric": "serving windows/s at 80% load, p50/p99 job latency", "value": value,
+                          "unit": "windows/s", "impl": "reference", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+                          "data": "synthetic (seeded)", "config": {"workload": "config 4 serving loop",
+                                                                   "jobs": len(jobs)},
+                          "cpu_baseline": {"value": value, "unit": "windows/s", "cores": threads, "kind": "port",
+                                           "sample": "jobs polished back to back until 30 s (CPU oracle)"},
+                          "e2e": {"value": value, "unit": "windows/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
     paths = _data(args, 0)
     wins = oracle.dump_windows(*paths, threads=os.cpu_count() or 1)
     n_sample = min(args.cpu_sample, len(wins))
@@ -188,6 +299,20 @@ def main():
     import racon_b200
     world, rank, local = _dist()
     torch.cuda.set_device(local)
+    if args.config == 4:
+        # serving loop alone: load sweep over the config-4 job stream
+        res = run_serving(args, local, [0.25, 0.5, 0.8, 1.0])
+        best = max(r["windows_per_s"] for r in res["rates"])
+        r80 = [r for r in res["rates"] if r["load"] == 0.8][0]
+        if rank == 0:
+            print(json.dumps({"metric": "serving windows/s at 80% load, p50/p99 job latency", "value": r80["windows_per_s"],
+                              "unit": "windows/s", "n_gpus": world, "steps": 1, "warmup": 1,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+                              "data": "synthetic (seeded)", "config": {"workload": "config 4 serving loop",
+                                                                       "jobs": res["jobs"]},
+                              "p99_latency_vs_isolated": r80["latency_vs_isolated"]["p99"],
+                              "best_windows_per_s": best, "serving": res}))
+        return
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
@@ -317,10 +442,13 @@ def main():
                                "gcups": ccells / sec / 1e9,
                                "sample": "first %d of %d windows, one pass (CPU oracle restatement of racon's "
                                          "algorithm; reference racon does not build here)" % (n, n_win)}
-    if rank == 0:
-        print(json.dumps(out))
     ctx.close()
     job.close()
+    if world == 1 and args.serving_jobs > 0:
+        # config 4 serving loop at 80% of its measured peak (--config 4 sweeps the load)
+        out["serving"] = run_serving(args, local, [0.8])
+    if rank == 0:
+        print(json.dumps(out))
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -223,6 +223,66 @@ size_t rb_job_windows(const rb_job* job, const rb_window** windows);
 void rb_job_free(rb_job* job);
 void rb_free(void* p);
 
+/* ---------------------------------------------------------------------
+ * Serving loop (no counterpart in the reference, which polishes one job per
+ * process): polishing jobs are submitted while others run.
+ * ------------------------------------------------------------------- */
+
+/* workers: jobs in flight at once. Each worker owns one long-lived device
+ * context with its own stream, so device buffers stay allocated from job to
+ * job and concurrent jobs' kernels overlap on the GPU. hbm_budget: device
+ * bytes the jobs in flight may take by estimate; a queued job is admitted,
+ * first in first out, when a worker is idle and its estimated footprint fits
+ * beside the jobs in flight (a job alone is always admitted). Each worker's
+ * window-consensus scratch is also capped at hbm_budget / workers. 0 selects
+ * 4 workers and 75% of the device memory. */
+typedef struct rb_server_params {
+    int device;
+    uint32_t workers;
+    uint64_t hbm_budget;
+    int8_t match;
+    int8_t mismatch;
+    int8_t gap;
+    uint32_t window_length;
+} rb_server_params;
+
+/* One job: racon's inputs and per-job flags (-f, -q, -e, --no-trimming, -u). */
+typedef struct rb_server_job {
+    const char* sequences_path;
+    const char* overlaps_path;
+    const char* target_path;
+    int fragment;
+    double quality_threshold;
+    double error_threshold;
+    int trim;
+    int drop_unpolished;
+} rb_server_job;
+
+/* Times of one job in seconds on the server's clock (0 = creation), its
+ * estimated footprint and the worker that ran it. */
+typedef struct rb_server_times {
+    double submitted, admitted, finished;
+    double stage_seconds[4];  /* load, align, layers, consensus */
+    uint64_t footprint;
+    uint32_t worker;
+} rb_server_times;
+
+typedef struct rb_server rb_server;
+/* Returns NULL on failure; rb_create_error() then holds the reason. */
+rb_server* rb_server_create(const rb_server_params* params);
+/* Queues a job (paths are copied) and returns its ticket. */
+int rb_server_submit(rb_server* server, const rb_server_job* job, uint64_t* ticket);
+/* Waits for a job. On RB_OK *fasta holds the polished FASTA text (malloc,
+ * free with rb_free); on failure *fasta is NULL and rb_server_error() holds
+ * the message. times may be NULL. A ticket can be waited for once. */
+int rb_server_wait(rb_server* server, uint64_t ticket, char** fasta, rb_server_times* times);
+/* Message of the calling thread's last failed rb_server_submit / _wait. */
+const char* rb_server_error(void);
+/* Jobs queued and in flight. */
+int rb_server_load(rb_server* server, uint32_t* queued, uint32_t* in_flight, uint64_t* in_flight_bytes);
+/* Cancels queued jobs, waits for the jobs in flight and frees the server. */
+void rb_server_destroy(rb_server* server);
+
 /* Edit distance of one pair (edlib NW semantics, the same value as
  * rb_align_batch's edit_distance) that allocates no memory. No counterpart in
  * the reference: racon always aligns through edlibAlign, which allocates.

@@ -73,6 +73,24 @@ class _PoaResult(ctypes.Structure):
                 ("polished", ctypes.POINTER(ctypes.c_uint8))]
 
 
+class _ServerParams(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
+                ("match", ctypes.c_int8), ("mismatch", ctypes.c_int8), ("gap", ctypes.c_int8),
+                ("window_length", ctypes.c_uint32)]
+
+
+class _ServerJob(ctypes.Structure):
+    _fields_ = [("sequences_path", ctypes.c_char_p), ("overlaps_path", ctypes.c_char_p),
+                ("target_path", ctypes.c_char_p), ("fragment", ctypes.c_int),
+                ("quality_threshold", ctypes.c_double), ("error_threshold", ctypes.c_double),
+                ("trim", ctypes.c_int), ("drop_unpolished", ctypes.c_int)]
+
+
+class ServerTimes(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_double), ("admitted", ctypes.c_double), ("finished", ctypes.c_double),
+                ("stage_seconds", ctypes.c_double * 4), ("footprint", ctypes.c_uint64), ("worker", ctypes.c_uint32)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("launches", ctypes.c_uint64),
@@ -127,6 +145,14 @@ def load():
     lib.rb_job_windows.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(_Window))]
     lib.rb_job_free.argtypes = [vp]
     lib.rb_free.argtypes = [vp]
+    lib.rb_server_create.restype = vp
+    lib.rb_server_create.argtypes = [ctypes.POINTER(_ServerParams)]
+    lib.rb_server_submit.argtypes = [vp, ctypes.POINTER(_ServerJob), ctypes.POINTER(ctypes.c_uint64)]
+    lib.rb_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ServerTimes)]
+    lib.rb_server_error.restype = ctypes.c_char_p
+    lib.rb_server_load.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                                   ctypes.POINTER(ctypes.c_uint64)]
+    lib.rb_server_destroy.argtypes = [vp]
     _lib = lib
     return lib
 
@@ -378,3 +404,65 @@ class Job:
             bb += w.backbone_length
             lb += sum(w.layer_lengths[j] for j in range(w.n_layers))
         return self.n, nl, lb, bb
+
+
+class Server:
+    """Serving loop (rb_server_*): polishing jobs submitted while others run.
+
+    workers jobs run at once, each on a long-lived device context of its own;
+    queued jobs are admitted first in first out when a worker is idle and the
+    job's estimated device footprint fits in hbm_budget beside the jobs in
+    flight. submit() returns a ticket; wait(ticket) returns (fasta, times)."""
+
+    def __init__(self, device=0, workers=4, hbm_budget=0, match=3, mismatch=-5, gap=-4, window_length=500):
+        self.lib = load()
+        p = _ServerParams(device, workers, hbm_budget, match, mismatch, gap, window_length)
+        self.ptr = self.lib.rb_server_create(ctypes.byref(p))
+        if not self.ptr:
+            raise RaconB200Error(5, self.lib.rb_create_error().decode())
+
+    def submit(self, sequences, overlaps, targets, fragment=False, quality_threshold=10.0, error_threshold=0.3,
+               trim=True, drop_unpolished=True):
+        j = _ServerJob(_b(sequences), _b(overlaps), _b(targets), int(fragment), quality_threshold,
+                       error_threshold, int(trim), int(drop_unpolished))
+        t = ctypes.c_uint64()
+        rc = self.lib.rb_server_submit(self.ptr, ctypes.byref(j), ctypes.byref(t))
+        if rc != RB_OK:
+            raise RaconB200Error(rc, self.lib.rb_server_error().decode())
+        return t.value
+
+    def wait(self, ticket):
+        out = ctypes.c_void_p()
+        tm = ServerTimes()
+        rc = self.lib.rb_server_wait(self.ptr, ticket, ctypes.byref(out), ctypes.byref(tm))
+        if rc != RB_OK:
+            raise RaconB200Error(rc, self.lib.rb_server_error().decode())
+        try:
+            text = ctypes.string_at(out.value).decode()
+        finally:
+            self.lib.rb_free(out)
+        return text, {"submitted": tm.submitted, "admitted": tm.admitted, "finished": tm.finished,
+                      "stage_seconds": list(tm.stage_seconds), "footprint": tm.footprint, "worker": tm.worker}
+
+    def load(self):
+        q, f, b = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint64()
+        self.lib.rb_server_load(self.ptr, ctypes.byref(q), ctypes.byref(f), ctypes.byref(b))
+        return q.value, f.value, b.value
+
+    def close(self):
+        if self.ptr:
+            self.lib.rb_server_destroy(self.ptr)
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

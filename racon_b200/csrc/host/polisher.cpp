@@ -430,6 +430,31 @@ public:
 
 // ---------------------------------------------------------------- Polisher
 
+// Argument checks of createPolisher (src/polisher.cpp:135-159): polisher
+// type, window length and the three file extensions.
+static void check_polisher_args(const std::string& sequences_path, const std::string& overlaps_path,
+                         const std::string& target_path, PolisherType type, uint32_t window_length, int& sf,
+                         int& of, int& tf) {
+    if (type != PolisherType::kC && type != PolisherType::kF)
+        fail("[racon::createPolisher] error: invalid polisher type!");
+    if (window_length == 0) fail("[racon::createPolisher] error: invalid window length!");
+    sf = sequence_format(sequences_path);
+    if (sf < 0)
+        fail("[racon::createPolisher] error: file " + sequences_path +
+             " has unsupported format extension (valid extensions: .fasta, .fasta.gz, .fna, .fna.gz, "
+             ".fa, .fa.gz, .fastq, .fastq.gz, .fq, .fq.gz)!");
+    of = overlap_format(overlaps_path);
+    if (of < 0)
+        fail("[racon::createPolisher] error: file " + overlaps_path +
+             " has unsupported format extension (valid extensions: .mhap, .mhap.gz, .paf, .paf.gz, "
+             ".sam, .sam.gz)!");
+    tf = sequence_format(target_path);
+    if (tf < 0)
+        fail("[racon::createPolisher] error: file " + target_path +
+             " has unsupported format extension (valid extensions: .fasta, .fasta.gz, .fna, .fna.gz, "
+             ".fa, .fa.gz, .fastq, .fastq.gz, .fq, .fq.gz)!");
+}
+
 std::unique_ptr<Polisher> createPolisher(const std::string& sequences_path,
     const std::string& overlaps_path, const std::string& target_path,
     PolisherType type, uint32_t window_length, double quality_threshold,
@@ -440,37 +465,38 @@ std::unique_ptr<Polisher> createPolisher(const std::string& sequences_path,
     (void)cuda_banded_alignment;
     (void)cudaaligner_batches;
     (void)cudaaligner_band_width;
-    if (type != PolisherType::kC && type != PolisherType::kF)
-        fail("[racon::createPolisher] error: invalid polisher type!");
-    if (window_length == 0) fail("[racon::createPolisher] error: invalid window length!");
-    const int sf = sequence_format(sequences_path);
-    if (sf < 0)
-        fail("[racon::createPolisher] error: file " + sequences_path +
-             " has unsupported format extension (valid extensions: .fasta, .fasta.gz, .fna, .fna.gz, "
-             ".fa, .fa.gz, .fastq, .fastq.gz, .fq, .fq.gz)!");
-    const int of = overlap_format(overlaps_path);
-    if (of < 0)
-        fail("[racon::createPolisher] error: file " + overlaps_path +
-             " has unsupported format extension (valid extensions: .mhap, .mhap.gz, .paf, .paf.gz, "
-             ".sam, .sam.gz)!");
-    const int tf = sequence_format(target_path);
-    if (tf < 0)
-        fail("[racon::createPolisher] error: file " + target_path +
-             " has unsupported format extension (valid extensions: .fasta, .fasta.gz, .fna, .fna.gz, "
-             ".fa, .fa.gz, .fastq, .fastq.gz, .fq, .fq.gz)!");
+    int sf, of, tf;
+    check_polisher_args(sequences_path, overlaps_path, target_path, type, window_length, sf, of, tf);
     return std::unique_ptr<Polisher>(new Polisher(sequences_path, overlaps_path, target_path, sf, of, tf, type,
                                                   window_length, quality_threshold, error_threshold, trim,
                                                   match, mismatch, gap, num_threads));
 }
 
+std::unique_ptr<Polisher> createPolisherOnContext(rb_ctx* ctx, int device, const std::string& sequences_path,
+    const std::string& overlaps_path, const std::string& target_path, PolisherType type, uint32_t window_length,
+    double quality_threshold, double error_threshold, bool trim, int8_t match, int8_t mismatch, int8_t gap) {
+    if (!ctx) fail("[racon::createPolisher] error: no device context!");
+    int sf, of, tf;
+    check_polisher_args(sequences_path, overlaps_path, target_path, type, window_length, sf, of, tf);
+    return std::unique_ptr<Polisher>(new Polisher(sequences_path, overlaps_path, target_path, sf, of, tf, type,
+                                                  window_length, quality_threshold, error_threshold, trim,
+                                                  match, mismatch, gap, 1, ctx, device));
+}
+
 Polisher::Polisher(const std::string& sp, const std::string& op, const std::string& tp, int sf, int of,
                    int tf, PolisherType type, uint32_t window_length, double quality_threshold,
                    double error_threshold, bool trim, int8_t match, int8_t mismatch, int8_t gap,
-                   uint32_t num_threads)
+                   uint32_t num_threads, rb_ctx* borrowed_ctx, int device)
     : sequences_path_(sp), overlaps_path_(op), target_path_(tp), sequences_format_(sf),
       overlaps_format_(of), target_format_(tf), type_(type), quality_threshold_(quality_threshold),
       error_threshold_(error_threshold), trim_(trim), match_(match), mismatch_(mismatch), gap_(gap),
       dummy_quality_(window_length, '!'), window_length_(window_length), num_threads_(num_threads) {
+    if (borrowed_ctx) {
+        ctx_ = borrowed_ctx;
+        owns_ctx_ = false;
+        device_ = device;
+        return;
+    }
     const char* dev = getenv("RACON_B200_DEVICE");
     device_ = dev ? atoi(dev) : 0;
     rb_params p;
@@ -483,7 +509,7 @@ Polisher::Polisher(const std::string& sp, const std::string& op, const std::stri
 }
 
 Polisher::~Polisher() {
-    if (ctx_) rb_destroy(ctx_);
+    if (ctx_ && owns_ctx_) rb_destroy(ctx_);
 }
 
 void Polisher::initialize() {
@@ -766,6 +792,41 @@ std::vector<std::unique_ptr<Sequence>> polish_files(const std::string& sp, const
     if (stage_seconds)
         for (int i = 0; i < 4; ++i) stage_seconds[i] = p->stage_seconds()[i];
     return out;
+}
+
+int polish_job_on_context(rb_ctx* ctx, int device, const std::string& sp, const std::string& op,
+                          const std::string& tp, bool fragment, uint32_t w, double q, double e, bool trim,
+                          int8_t m, int8_t x, int8_t g, bool drop, std::string* fasta, std::string* error,
+                          double* stage_seconds) {
+    const bool was = g_throw_on_error;
+    g_throw_on_error = true;
+    try {
+        auto p = createPolisherOnContext(ctx, device, sp, op, tp, fragment ? PolisherType::kF : PolisherType::kC, w,
+                                         q, e, trim, m, x, g);
+        p->initialize();
+        std::vector<std::unique_ptr<Sequence>> out;
+        p->polish(out, drop);
+        if (stage_seconds)
+            for (int i = 0; i < 4; ++i) stage_seconds[i] = p->stage_seconds()[i];
+        fasta->clear();
+        for (const auto& r : out) {
+            *fasta += '>';
+            *fasta += r->name();
+            *fasta += '\n';
+            *fasta += r->data();
+            *fasta += '\n';
+        }
+        g_throw_on_error = was;
+        return RB_OK;
+    } catch (const Fatal& ex) {
+        g_throw_on_error = was;
+        *error = ex.what();
+        return RB_ERR_ARG;
+    } catch (const std::bad_alloc&) {
+        g_throw_on_error = was;
+        *error = "host allocation failed";
+        return RB_ERR_NOMEM;
+    }
 }
 
 }  // namespace racon

@@ -90,13 +90,19 @@ public:
         uint32_t num_threads, uint32_t cuda_batches, bool cuda_banded_alignment,
         uint32_t cudaaligner_batches, uint32_t cudaaligner_band_width);
     friend struct ::rb_job;
+    friend std::unique_ptr<Polisher> createPolisherOnContext(rb_ctx* ctx, int device,
+        const std::string& sequences_path, const std::string& overlaps_path,
+        const std::string& target_path, PolisherType type, uint32_t window_length,
+        double quality_threshold, double error_threshold, bool trim, int8_t match,
+        int8_t mismatch, int8_t gap);
 
 protected:
     Polisher(const std::string& sequences_path, const std::string& overlaps_path,
         const std::string& target_path, int sequences_format, int overlaps_format,
         int target_format, PolisherType type, uint32_t window_length,
         double quality_threshold, double error_threshold, bool trim, int8_t match,
-        int8_t mismatch, int8_t gap, uint32_t num_threads);
+        int8_t mismatch, int8_t gap, uint32_t num_threads, rb_ctx* borrowed_ctx = nullptr,
+        int device = 0);
     Polisher(const Polisher&) = delete;
     const Polisher& operator=(const Polisher&) = delete;
     virtual void find_overlap_breaking_points(std::vector<std::unique_ptr<Overlap>>& overlaps);
@@ -121,8 +127,30 @@ protected:
     uint32_t num_threads_;
     int device_ = 0;
     rb_ctx* ctx_ = nullptr;
+    bool owns_ctx_ = true;
     double stage_s_[4] = {0, 0, 0, 0};
 };
+
+// Not part of racon's API: a polisher that runs on an existing context
+// (created with the same match / mismatch / gap / window length), which it
+// does not destroy. The serving loop gives each worker one long-lived
+// context so that device buffers stay allocated from job to job.
+std::unique_ptr<Polisher> createPolisherOnContext(rb_ctx* ctx, int device,
+    const std::string& sequences_path, const std::string& overlaps_path,
+    const std::string& target_path, PolisherType type, uint32_t window_length,
+    double quality_threshold, double error_threshold, bool trim, int8_t match,
+    int8_t mismatch, int8_t gap);
+
+// One polishing job on a borrowed context, with racon's fatal errors turned
+// into a return value: RB_OK and the FASTA text (">name tags\nsequence\n"
+// records), or RB_ERR_ARG and the "[racon::...] error: ..." message.
+// stage_seconds (may be NULL) receives load, align, layers and consensus
+// seconds. Used by the serving loop.
+int polish_job_on_context(rb_ctx* ctx, int device, const std::string& sequences_path,
+    const std::string& overlaps_path, const std::string& target_path, bool fragment,
+    uint32_t window_length, double quality_threshold, double error_threshold, bool trim,
+    int8_t match, int8_t mismatch, int8_t gap, bool drop_unpolished, std::string* fasta,
+    std::string* error, double* stage_seconds);
 
 // Creates the polisher and runs initialize + polish; used by the CLI and the
 // C entry point rb_polish_files. Returns the polished records.

@@ -1,0 +1,279 @@
+// Serving loop over the B200 polishing path (include/racon_b200.h,
+// rb_server_*). racon itself polishes one job per process; this keeps a pool
+// of device contexts alive and runs jobs as they arrive.
+//
+// Design:
+//   - `workers` threads, each owning one rb_ctx (own CUDA stream, own device
+//     buffers). Buffers grow to the largest job a worker has run and stay
+//     allocated, so a steady stream of jobs does no cudaMalloc / cudaFree
+//     (which would synchronise the device and stall the other workers).
+//   - Jobs on different workers overlap on the device: one job's host stages
+//     (parsing, layer assembly, stitching) run while another's kernels run,
+//     and the kernels of concurrent jobs share the SMs as CTAs retire.
+//   - Admission is first in first out by estimated device footprint: the
+//     head of the queue starts when a worker is idle and its estimate fits
+//     beside the jobs in flight within hbm_budget (a job alone always
+//     starts). Each worker's window-consensus scratch is capped at
+//     hbm_budget / workers, which bounds the real allocation too.
+#include <cuda_runtime.h>
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../../include/racon_b200.h"
+#include "../rb_internal.hpp"
+#include "racon.hpp"
+
+namespace {
+
+thread_local std::string t_server_error;
+
+struct Request {
+    uint64_t ticket = 0;
+    std::string sp, op, tp;
+    rb_server_job spec{};
+    uint64_t footprint = 0;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    double stage[4] = {0, 0, 0, 0};
+    uint32_t worker = 0;
+    bool done = false;
+    int status = RB_OK;
+    std::string fasta, error;
+};
+
+uint64_t file_bytes(const std::string& p) {
+    struct stat st;
+    if (stat(p.c_str(), &st) != 0) return 0;
+    const uint64_t b = uint64_t(st.st_size);
+    const size_t n = p.size();
+    // gzip'd inputs expand roughly fourfold
+    return (n > 3 && p.compare(n - 3, 3, ".gz") == 0) ? 4 * b : b;
+}
+
+}  // namespace
+
+struct rb_server {
+    rb_server_params params{};
+    int sm_count = 148;
+    uint64_t poa_cap = 0;
+    std::vector<rb_ctx*> ctxs;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<Request>> queue;
+    std::map<uint64_t, std::shared_ptr<Request>> jobs;
+    uint64_t next_ticket = 1;
+    uint64_t inflight_bytes = 0;
+    uint32_t inflight = 0;
+    bool stop = false;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    // Device bytes a job is expected to hold: its inputs on the device, the
+    // alignment scratch and one consensus slot per resident window.
+    uint64_t estimate(const Request& r) const {
+        const uint64_t reads = file_bytes(r.sp), targets = file_bytes(r.tp);
+        const uint64_t w = std::max<uint32_t>(1, params.window_length);
+        const uint64_t windows = targets / w + 1;
+        const uint64_t resident = std::min<uint64_t>(windows, uint64_t(sm_count) * 12);
+        const uint64_t slot = rb::PoaEngine::slot_bytes_for(uint32_t(std::min<uint64_t>(3 * w, 65535)));
+        const uint64_t poa = std::min<uint64_t>(resident * slot, poa_cap);
+        const uint64_t align = std::min<uint64_t>(uint64_t(4) << 30, (reads + targets) * 8 + (uint64_t(256) << 20));
+        return poa + align + 3 * (reads + targets);
+    }
+
+    bool admissible(const Request& r) const {
+        return inflight == 0 || inflight_bytes + r.footprint <= params.hbm_budget;
+    }
+
+    void worker(uint32_t w) {
+        cudaSetDevice(params.device);
+        while (true) {
+            std::shared_ptr<Request> r;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] { return stop || (!queue.empty() && admissible(*queue.front())); });
+                if (stop) return;
+                r = queue.front();
+                queue.pop_front();
+                inflight_bytes += r->footprint;
+                ++inflight;
+                r->t_admit = now();
+                r->worker = w;
+            }
+            cv_work.notify_all();
+            std::string fasta, error;
+            double stage[4] = {0, 0, 0, 0};
+            const rb_server_job& j = r->spec;
+            const int rc = racon::polish_job_on_context(
+                ctxs[w], params.device, r->sp, r->op, r->tp, j.fragment != 0, params.window_length,
+                j.quality_threshold, j.error_threshold, j.trim != 0, params.match, params.mismatch, params.gap,
+                j.drop_unpolished != 0, &fasta, &error, stage);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                inflight_bytes -= r->footprint;
+                --inflight;
+                r->status = rc;
+                r->fasta.swap(fasta);
+                r->error.swap(error);
+                for (int i = 0; i < 4; ++i) r->stage[i] = stage[i];
+                r->t_done = now();
+                r->done = true;
+            }
+            cv_done.notify_all();
+            cv_work.notify_all();
+        }
+    }
+};
+
+extern "C" {
+
+rb_server* rb_server_create(const rb_server_params* params) {
+    if (!params) return nullptr;
+    std::unique_ptr<rb_server> s(new rb_server());
+    s->params = *params;
+    if (s->params.workers == 0) s->params.workers = 4;
+    rb_params p;
+    p.match = params->match;
+    p.mismatch = params->mismatch;
+    p.gap = params->gap;
+    p.window_length = params->window_length;
+    for (uint32_t i = 0; i < s->params.workers; ++i) {
+        rb_ctx* c = rb_create(params->device, &p);
+        if (!c) {
+            for (rb_ctx* x : s->ctxs) rb_destroy(x);
+            return nullptr;  // rb_create_error() holds the reason
+        }
+        s->ctxs.push_back(c);
+    }
+    cudaSetDevice(params->device);
+    cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, params->device);
+    if (s->params.hbm_budget == 0) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        s->params.hbm_budget = uint64_t(total_b) / 4 * 3;
+    }
+    s->poa_cap = s->params.hbm_budget / s->params.workers;
+    for (rb_ctx* c : s->ctxs) rb::ctx_set_poa_budget(c, s->poa_cap);
+    for (uint32_t i = 0; i < s->params.workers; ++i) s->threads.emplace_back([srv = s.get(), i] { srv->worker(i); });
+    return s.release();
+}
+
+int rb_server_submit(rb_server* s, const rb_server_job* job, uint64_t* ticket) {
+    if (!s || !job || !ticket || !job->sequences_path || !job->overlaps_path || !job->target_path) {
+        t_server_error = "rb_server_submit: NULL argument";
+        return RB_ERR_ARG;
+    }
+    auto r = std::make_shared<Request>();
+    r->sp = job->sequences_path;
+    r->op = job->overlaps_path;
+    r->tp = job->target_path;
+    r->spec = *job;
+    r->spec.sequences_path = r->sp.c_str();
+    r->spec.overlaps_path = r->op.c_str();
+    r->spec.target_path = r->tp.c_str();
+    r->footprint = s->estimate(*r);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) {
+            t_server_error = "rb_server_submit: server is stopping";
+            return RB_ERR_ARG;
+        }
+        r->ticket = s->next_ticket++;
+        r->t_submit = s->now();
+        s->jobs[r->ticket] = r;
+        s->queue.push_back(r);
+        *ticket = r->ticket;
+    }
+    s->cv_work.notify_all();
+    return RB_OK;
+}
+
+int rb_server_wait(rb_server* s, uint64_t ticket, char** fasta, rb_server_times* times) {
+    if (!s || !fasta) {
+        t_server_error = "rb_server_wait: NULL argument";
+        return RB_ERR_ARG;
+    }
+    *fasta = nullptr;
+    std::shared_ptr<Request> r;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        auto it = s->jobs.find(ticket);
+        if (it == s->jobs.end()) {
+            t_server_error = "rb_server_wait: unknown ticket";
+            return RB_ERR_ARG;
+        }
+        r = it->second;
+        s->cv_done.wait(lk, [&] { return r->done; });
+        s->jobs.erase(it);
+    }
+    if (times) {
+        times->submitted = r->t_submit;
+        times->admitted = r->t_admit;
+        times->finished = r->t_done;
+        for (int i = 0; i < 4; ++i) times->stage_seconds[i] = r->stage[i];
+        times->footprint = r->footprint;
+        times->worker = r->worker;
+    }
+    if (r->status != RB_OK) {
+        t_server_error = r->error;
+        return r->status;
+    }
+    char* buf = static_cast<char*>(malloc(r->fasta.size() + 1));
+    if (!buf) {
+        t_server_error = "host allocation failed";
+        return RB_ERR_NOMEM;
+    }
+    memcpy(buf, r->fasta.c_str(), r->fasta.size() + 1);
+    *fasta = buf;
+    return RB_OK;
+}
+
+const char* rb_server_error(void) { return t_server_error.c_str(); }
+
+int rb_server_load(rb_server* s, uint32_t* queued, uint32_t* in_flight, uint64_t* in_flight_bytes) {
+    if (!s) return RB_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (queued) *queued = uint32_t(s->queue.size());
+    if (in_flight) *in_flight = s->inflight;
+    if (in_flight_bytes) *in_flight_bytes = s->inflight_bytes;
+    return RB_OK;
+}
+
+void rb_server_destroy(rb_server* s) {
+    if (!s) return;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        // cancel what has not started; let the jobs in flight finish
+        for (auto& r : s->queue) {
+            r->status = RB_ERR_ARG;
+            r->error = "rb_server: job cancelled (server destroyed)";
+            r->t_done = s->now();
+            r->done = true;
+        }
+        s->queue.clear();
+        s->cv_done.notify_all();
+        s->cv_done.wait(lk, [&] { return s->inflight == 0; });
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->threads) t.join();
+    for (rb_ctx* c : s->ctxs) rb_destroy(c);
+    delete s;
+}
+
+}  // extern "C"

@@ -1430,6 +1430,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, 3) poa_plain_kernel(PoaArgs
 
 }  // namespace
 
+size_t PoaEngine::slot_bytes_for(uint32_t max_layer_length) {
+    const int ncap = 4096;
+    return walk_layout(ncap, 2 * ncap, ncap, row_cover(int(max_layer_length) + 1), [](int, size_t) {});
+}
+
 PoaEngine::PoaEngine(const DeviceInfo& dev, cudaStream_t stream, int8_t m, int8_t x, int8_t g)
     : dev_(dev), stream_(stream), match_(m), mismatch_(x), gap_(g) {
     check_cuda(cudaEventCreate(&ev0_), "cudaEventCreate");
@@ -1603,7 +1608,7 @@ void PoaEngine::run(bool plain) {
         const size_t slot = walk_layout(ncap, ecap, acap, lcap, [](int, size_t) {});
         // resident windows (one warp each): enough to fill the SMs, bounded by
         // a scratch budget
-        const size_t budget = size_t(48) << 30;
+        const size_t budget = scratch_budget_;
         size_t slots = std::min<size_t>(todo.size(), plain ? todo.size() : size_t(dev_.sm_count) * 12);
         // RB_POA_SLOTS caps the resident windows (smaller scratch, e.g. for
         // profiler captures); results do not depend on it

@@ -57,6 +57,12 @@ struct rb_ctx {
     std::string err;
 };
 
+namespace rb {
+void ctx_set_poa_budget(rb_ctx* ctx, size_t bytes) {
+    if (ctx && ctx->poa) ctx->poa->set_scratch_budget(bytes);
+}
+}  // namespace rb
+
 namespace {
 std::mutex g_err_mu;
 std::string g_create_err;

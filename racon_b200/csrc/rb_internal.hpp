@@ -100,6 +100,11 @@ public:
     void run(bool plain = false);
     void fetch(rb_poa_result* out);
     const rb_stats& stats() const { return stats_; }
+    // device bytes the per-window scratch slots may take (resident windows
+    // are halved until they fit)
+    void set_scratch_budget(size_t bytes) { scratch_budget_ = bytes; }
+    // scratch bytes of one resident window at the starting graph capacity
+    static size_t slot_bytes_for(uint32_t max_layer_length);
 
 private:
     DeviceInfo dev_;
@@ -118,7 +123,12 @@ private:
     std::vector<char> cons_;
     std::vector<uint8_t> polished_;
     std::vector<std::pair<uint64_t, uint32_t>> labels_;  // (id, rank) per window
+    size_t scratch_budget_ = size_t(48) << 30;
     rb_stats stats_{};
 };
+
+// Caps the window-consensus scratch of a context (server workers share one
+// device); defined in rb_capi.cpp.
+void ctx_set_poa_budget(rb_ctx* ctx, size_t bytes);
 
 }  // namespace rb

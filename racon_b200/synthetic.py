@@ -17,6 +17,8 @@ unless given):
                 query = span mutated at 7% sub + 4% ins + 4% del, half reverse
                 complemented (the query is given in the orientation racon
                 aligns, so the pair itself is forward).
+  serving_jobs(...) config 4 job stream: config-0-like jobs with log-uniform
+                contig length, uniform coverage and error.
   fragment(...) read correction (config 3 shape, scaled): contigs, reads at a
                 sinusoidal local depth, all-vs-all PAF overlaps (dual
                 directions) from the known coordinates.
@@ -75,10 +77,11 @@ CONFIGS = {
 }
 
 
-def contig(out_dir, config=1, seed=None, scale=1.0, qual_range=(5, 30)):
+def contig(out_dir, config=1, seed=None, scale=1.0, qual_range=(5, 30), params=None):
     """Writes reads (FASTA/FASTQ), overlaps (PAF) and the draft (FASTA) of a
-    contig-polishing job; returns the three paths and a summary dict."""
-    c = dict(CONFIGS[config])
+    contig-polishing job; returns the three paths and a summary dict.
+    params (optional) replaces the configuration's shape dict."""
+    c = dict(CONFIGS[config] if params is None else params)
     rng = np.random.default_rng(config if seed is None else seed)
     g = max(2_000, int(c["genome"] * scale))
     truth = rng.integers(0, 4, g, dtype=np.uint8)
@@ -124,6 +127,27 @@ def contig(out_dir, config=1, seed=None, scale=1.0, qual_range=(5, 30)):
         tf.write(b">draft\n" + BASES[draft].tobytes() + b"\n")
     info = {"config": config, "genome": g, "reads": int(n_reads), "draft_length": dlen}
     return rpath, opath, tpath, info
+
+
+def serving_jobs(out_dir, count, seed=4, length=(20_000, 2_000_000), coverage=(20, 80), error=(0.08, 0.15)):
+    """Config 4 job stream: `count` config-0-like jobs with contig length
+    log-uniform in `length`, coverage uniform in `coverage` and read error
+    uniform in `error` (split 5:4:4 over sub/ins/del as in config 0). Returns
+    a list of (reads, overlaps, draft, info), job i generated from seed
+    (seed, i)."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(count):
+        g = int(np.exp(rng.uniform(np.log(length[0]), np.log(length[1]))))
+        cov = float(rng.uniform(*coverage))
+        err = float(rng.uniform(*error))
+        params = dict(CONFIGS[0])
+        params.update(genome=g, coverage=cov, read_err=(err * 5 / 13, err * 4 / 13, err * 4 / 13))
+        d = os.path.join(out_dir, "job%03d" % i)
+        r, o, t, info = contig(d, 0, seed=int(rng.integers(1 << 31)), params=params)
+        info.update(coverage=cov, error=err)
+        jobs.append((r, o, t, info))
+    return jobs
 
 
 def pairs(count, lo=1_000, hi=50_000, seed=2, err=(0.07, 0.04, 0.04)):

@@ -1,0 +1,57 @@
+"""Serving loop (rb_server_*): every job's FASTA is the same alone and in the
+mix, admission by footprint serialises jobs under a small budget, and a bad
+job fails alone without stopping the server."""
+import pytest
+
+from conftest import lambda_path
+
+pytestmark = pytest.mark.gpu
+
+# four of racon's golden jobs that share -m 5 -x -4 -g -8 -w 500
+JOBS = [
+    ("sample_reads.fastq.gz", "sample_overlaps.paf.gz"),
+    ("sample_reads.fasta.gz", "sample_overlaps.paf.gz"),
+    ("sample_reads.fastq.gz", "sample_overlaps.sam.gz"),
+    ("sample_reads.fasta.gz", "sample_overlaps.sam.gz"),
+]
+TARGET = "sample_layout.fasta.gz"
+
+
+def _alone(native_lib):
+    return [native_lib.polish_files(lambda_path(r), lambda_path(o), lambda_path(TARGET), match=5, mismatch=-4,
+                                    gap=-8) for r, o in JOBS]
+
+
+def test_server_mix_matches_alone(native_lib):
+    want = _alone(native_lib)
+    with native_lib.Server(0, workers=3, match=5, mismatch=-4, gap=-8, window_length=500) as srv:
+        tickets = [srv.submit(lambda_path(r), lambda_path(o), lambda_path(TARGET)) for r, o in JOBS * 2]
+        got = [srv.wait(t) for t in tickets]
+    for i, (fasta, times) in enumerate(got):
+        assert fasta == want[i % len(JOBS)], "job %d differs in the mix" % i
+        assert times["submitted"] <= times["admitted"] <= times["finished"]
+    # with 3 workers, some jobs overlapped in time
+    spans = sorted((t["admitted"], t["finished"]) for _, t in got)
+    assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+
+
+def test_server_budget_serialises(native_lib):
+    want = _alone(native_lib)[:2]
+    # a 1-byte budget admits one job at a time (a job alone always starts)
+    with native_lib.Server(0, workers=2, hbm_budget=1, match=5, mismatch=-4, gap=-8) as srv:
+        tickets = [srv.submit(lambda_path(r), lambda_path(o), lambda_path(TARGET)) for r, o in JOBS[:2] * 2]
+        got = [srv.wait(t) for t in tickets]
+    for i, (fasta, _) in enumerate(got):
+        assert fasta == want[i % 2]
+    spans = sorted((t["admitted"], t["finished"]) for _, t in got)
+    assert all(spans[i + 1][0] >= spans[i][1] for i in range(len(spans) - 1))
+
+
+def test_server_bad_job_fails_alone(native_lib):
+    want = _alone(native_lib)[0]
+    with native_lib.Server(0, workers=2, match=5, mismatch=-4, gap=-8) as srv:
+        bad = srv.submit(lambda_path("sample_reads.fastq.gz"), "/nonexistent/overlaps.txt", lambda_path(TARGET))
+        good = srv.submit(lambda_path(JOBS[0][0]), lambda_path(JOBS[0][1]), lambda_path(TARGET))
+        with pytest.raises(native_lib.RaconB200Error, match="unsupported format extension"):
+            srv.wait(bad)
+        assert srv.wait(good)[0] == want
