@@ -111,6 +111,19 @@ struct Graph {
 
 __host__ __device__ size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
+// Decision bytes are stored in tiles of 8 rows x 128 columns (1 KiB): a
+// warp still writes each row as whole 128-byte lines, and the traceback,
+// which walks up and left one cell at a time through nearby rows, stays
+// inside one tile for several steps. lc is a multiple of 128.
+__device__ __forceinline__ size_t dec_at(int i, int j, int lc) {
+    return size_t(i) * size_t(lc) + size_t(j);
+}
+
+// Row descriptor word w: predecessor count (17 bits) | sink << 17 | base << 24.
+__device__ __forceinline__ int desc_np(int w) { return w & 0x1FFFF; }
+__device__ __forceinline__ bool desc_sink(int w) { return (w >> 17) & 1; }
+__device__ __forceinline__ uint32_t desc_base(int w) { return uint32_t(w) >> 24; }
+
 struct SlotLayout {
     size_t bytes;
 };
@@ -156,7 +169,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(N * 4, 29);       // bpred
     take(N * 4, 30);       // cons
     take((N + 1) * L * 4, 31);  // H
-    take((N + 1) * L, 32);      // dec
+    take(((N + 8) & ~size_t(7)) * L, 32);  // dec, 8-row tiles
     take(N * 4, 33);       // ord
     take(N * 4, 34);       // ord2
     take(N * 4, 35);       // my_rank
@@ -683,6 +696,15 @@ __device__ int g_heaviest_bundle(const Graph& g, PoaShared& sh) {
     return len;
 }
 
+// Predecessor p (in in-edge order) of a DP row from its descriptor: DP rank
+// (0 = the empty prefix row when the row has no predecessor).
+__device__ __forceinline__ int desc_pred(const Graph& g, const int4& d, int p) {
+    const int np = desc_np(d.w);
+    if (np == 0) return 0;
+    if (np > 3) return g.pred_idx[d.x + p];
+    return p == 0 ? d.x : (p == 1 ? d.y : d.z);
+}
+
 // ---------------- DP of one layer (one warp) ----------------
 
 // Columns covered by one warp pass: S cells per lane, S a multiple of 4.
@@ -716,10 +738,6 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
     const int lc = g.lcap;
     int* const Hm = g.H;
     uint8_t* const Dm = g.dec;
-    const int* const pred_off = g.pred_off;
-    const int* const pred_idx = g.pred_idx;
-    const uint8_t* const sinkf = g.sink;
-    const uint8_t* const codes = g.code;
     const int wc = L + 1;
     const int ch = 32 * S;
     const int nch = (wc + ch - 1) / ch;
@@ -730,12 +748,11 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
     const int lane_l = (L % ch) / S, k_l = L % S, ch_l = L / ch;
     int best_v = kNegInf, best_r = INT_MAX, ties = 0;
     for (int i = 1; i <= ndp; ++i) {
-        const int v = order[i - 1];
-        const uint32_t cmask = uint32_t(codes[v]) * 0x01010101u;
-        const int pb = pred_off[i - 1], pe = pred_off[i];
-        const int np = pe - pb;
+        const int4 d = g.rowdesc[i - 1];
+        const uint32_t cmask = desc_base(d.w) * 0x01010101u;
+        const int np = desc_np(d.w);
         const int cnt = np == 0 ? 1 : np;
-        const bool is_sink = sinkf[i - 1] != 0;
+        const bool is_sink = desc_sink(d.w);
         int carry_in = kNegInf;  // final H of the last column of the previous chunk
         for (int c = 0; c < nch; ++c) {
             const int j0 = c * ch + lane * S;
@@ -760,7 +777,7 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
                 code[k] = 0xFFFFu;
             }
             for (int p = 0; p < cnt; ++p) {
-                const int r = np == 0 ? 0 : pred_idx[pb + p];
+                const int r = desc_pred(g, d, p);
                 const int4* hp4 = reinterpret_cast<const int4*>(Hm + r * lc + j0);
                 int hv[S];
 #pragma unroll
@@ -832,9 +849,8 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
 #pragma unroll
             for (int q = 0; q < S / 4; ++q)
                 out4[q] = make_int4(hrow[4 * q], hrow[4 * q + 1], hrow[4 * q + 2], hrow[4 * q + 3]);
-            uint32_t* d4 = reinterpret_cast<uint32_t*>(Dm + size_t(i) * lc + j0);
 #pragma unroll
-            for (int q = 0; q < S / 4; ++q) d4[q] = dec4[q];
+            for (int q = 0; q < S / 4; ++q) *reinterpret_cast<uint32_t*>(Dm + dec_at(i, j0 + 4 * q, lc)) = dec4[q];
             if (c == ch_l && lane == lane_l && is_sink) {
                 int val = kNegInf;
 #pragma unroll
@@ -858,6 +874,10 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
 }
 
 constexpr int kRingBytesPerWarp = 16384;
+// node ranks held in the ring's shared memory during the descriptor build
+constexpr int kSmemRanks = (kRingBytesPerWarp - 512) / 4;
+// row descriptors a lane keeps in registers between the two build passes
+constexpr int kDescPerLane = 4;
 // last 512 bytes of each warp's ring hold the 32-row descriptor block
 constexpr int kRingDescOffset = (kRingBytesPerWarp - 512) / 16;
 
@@ -916,9 +936,9 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
             pre = nx < ndp ? rowdesc[nx] : make_int4(0, 0, 0, 0);
         }
         const int4 d = dblk[bi];
-        const int np = d.w & 0xFF;
-        const bool is_sink = (d.w >> 8) & 1;
-        const uint32_t cmask = uint32_t((d.w >> 16) & 0xFF) * 0x01010101u;
+        const int np = desc_np(d.w);
+        const bool is_sink = desc_sink(d.w);
+        const uint32_t cmask = desc_base(d.w) * 0x01010101u;
         const int p0 = np > 3 ? pred_idx[d.x] : d.x;
         uint32_t eq[Q];
 #pragma unroll
@@ -1032,9 +1052,8 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
             dst_g[q] = v4;
             dst_r[q * 32] = v4;
         }
-        uint32_t* d4 = reinterpret_cast<uint32_t*>(Dm + size_t(i) * lc + j0);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) d4[q] = dec4[q];
+        for (int q = 0; q < Q; ++q) *reinterpret_cast<uint32_t*>(Dm + dec_at(i, j0 + 4 * q, lc)) = dec4[q];
         if (lane == lane_l && is_sink) {
             int val = kNegInf;
 #pragma unroll
@@ -1072,7 +1091,9 @@ __device__ EndCell dp_dispatch(const PoaArgs& a, const Graph& g, const int* orde
 // Walk back from (iend, L) over the decision bytes (lane 0). Writes the
 // sequence-consuming steps of the alignment (node id or -1 for an inserted
 // base, sequence position), end of path first; vertical steps (a graph node
-// against a gap) consume no position and add nothing to the graph.
+// against a gap) consume no position and add nothing to the graph. Each step
+// loads the cell's decision byte and its row's descriptor (independent
+// loads); the next row comes from the descriptor.
 __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const int* order, const uint8_t* seq,
                           int L, int iend) {
     const int lc = g.lcap;
@@ -1087,27 +1108,24 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             --j;
             continue;
         }
-        uint32_t code = g.dec[size_t(i) * lc + j];
-        const int pb = g.pred_off[i - 1], np = g.pred_off[i] - pb;
+        const int4 d = g.rowdesc[i - 1];
         const int v = order[i - 1];
+        uint32_t code = g.dec[dec_at(i, j, lc)];
+        const int np = desc_np(d.w);
         if (code == 255u) {  // predecessor index >= 63: decide again from H
             const int h = g.H[i * lc + j];
-            const int s = j > 0 ? (seq[j - 1] == g.code[v] ? a.match : a.mismatch) : 0;
+            const int s = j > 0 ? (uint32_t(seq[j - 1]) == desc_base(d.w) ? a.match : a.mismatch) : 0;
             const int cnt = np == 0 ? 1 : np;
             code = 128u;
             int pick = -1;
             if (j > 0)
-                for (int p = 0; p < cnt && pick < 0; ++p) {
-                    const int r = np == 0 ? 0 : g.pred_idx[pb + p];
-                    if (g.H[r * lc + j - 1] + s == h) pick = p;
-                }
+                for (int p = 0; p < cnt && pick < 0; ++p)
+                    if (g.H[desc_pred(g, d, p) * lc + j - 1] + s == h) pick = p;
             if (pick >= 0) {
                 code = 1000u + uint32_t(pick);
             } else {
-                for (int p = 0; p < cnt && pick < 0; ++p) {
-                    const int r = np == 0 ? 0 : g.pred_idx[pb + p];
-                    if (g.H[r * lc + j] + a.gap == h) pick = p;
-                }
+                for (int p = 0; p < cnt && pick < 0; ++p)
+                    if (g.H[desc_pred(g, d, p) * lc + j] + a.gap == h) pick = p;
                 if (pick >= 0) code = 2000u + uint32_t(pick);
             }
         }
@@ -1116,11 +1134,11 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             g.aln_node[n] = v;
             g.aln_pos[n] = j - 1;
             ++n;
-            i = np == 0 ? 0 : g.pred_idx[pb + p];
+            i = desc_pred(g, d, p);
             --j;
         } else if (code < 128u || code >= 2000u) {
             const int p = code < 128u ? int(code - 64u) : int(code - 2000u);
-            i = np == 0 ? 0 : g.pred_idx[pb + p];  // vertical: no sequence position
+            i = desc_pred(g, d, p);  // vertical: no sequence position
         } else {
             if (j == 0) return false;
             g.aln_node[n] = -1;
@@ -1201,7 +1219,6 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         const int N = sh.nnodes;
         for (int i = lane; i < N; i += 32) {
             g.member[i] = full ? 1 : 0;
-            g.dprank[i] = 0;
         }
         __syncwarp();
         if (lane == 0) {
@@ -1228,59 +1245,80 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
             order = g.dporder;
             __syncwarp();
         }
-        for (int i = lane; i < ndp; i += 32) g.dprank[order[i]] = i + 1;
+        // Row descriptors. DP ranks of the nodes live in shared memory (the
+        // row ring is free until the DP) when they fit, else in global
+        // scratch; bit 31 marks a node with a successor among the rows.
+        int* const dpr = N <= kSmemRanks ? reinterpret_cast<int*>(ring) : g.dprank;
+        for (int i = lane; i < N; i += 32) dpr[i] = 0;
         __syncwarp();
-        // predecessor counts (DP ranks, in in-edge order) and sinks
-        for (int i = lane; i < ndp; i += 32) {
-            const int v = order[i];
-            int cntp = 0;
-            for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e])
-                if (g.dprank[g.e_src[e]] > 0) ++cntp;
-            g.pred_off[i + 1] = cntp;
-            bool sink = true;
-            for (int e = g.out_head[v]; e != -1; e = g.e_next_out[e])
-                if (g.dprank[g.e_dst[e]] > 0) {
-                    sink = false;
-                    break;
-                }
-            g.sink[i] = sink ? 1 : 0;
-        }
+        for (int i = lane; i < ndp; i += 32) dpr[order[i]] = i + 1;
         __syncwarp();
-        // exclusive prefix of the counts (warp scan over chunks of 32)
-        {
-            int base = 0;
-            for (int c0 = 0; c0 < ndp; c0 += 32) {
-                const int i = c0 + lane;
-                int vcount = i < ndp ? g.pred_off[i + 1] : 0;
-                int incl = vcount;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                if (i < ndp) g.pred_off[i + 1] = base + incl;
-                base += __shfl_sync(0xffffffffu, incl, 31);
-            }
-            if (lane == 0) g.pred_off[0] = 0;
-        }
-        __syncwarp();
-        for (int i = lane; i < ndp; i += 32) {
-            const int v = order[i];
-            int k = g.pred_off[i];
-            const int k0 = k;
-            int pr[3] = {0, 0, 0};
+        // one pass over each row's in-edges (in-edge order = spoa's order):
+        // the first three predecessor ranks and the count, and the successor
+        // mark on every predecessor. The first 32 * kDescPerLane rows keep
+        // their partial descriptor in registers, the rest in global scratch.
+        auto scan_in_edges = [&](int v) {
+            int4 r4 = make_int4(0, 0, 0, 0);
             for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e]) {
-                const int r = g.dprank[g.e_src[e]];
+                const int src = g.e_src[e];
+                const int r = dpr[src] & 0x7FFFFFFF;
                 if (r > 0) {
-                    if (k - k0 < 3) pr[k - k0] = r;
-                    g.pred_idx[k++] = r;
+                    if (r4.w == 0) r4.x = r;
+                    else if (r4.w == 1) r4.y = r;
+                    else if (r4.w == 2) r4.z = r;
+                    ++r4.w;
+                    atomicOr(reinterpret_cast<unsigned*>(&dpr[src]), 0x80000000u);
                 }
             }
-            // descriptor: x,y,z = first predecessor ranks (x = list offset when
-            // more than three), w = count | sink << 8 | base << 16
-            const int np = k - k0;
-            g.rowdesc[i] = make_int4(np > 3 ? k0 : pr[0], pr[1], pr[2],
-                                     np | (int(g.sink[i]) << 8) | (int(g.code[v]) << 16));
+            return r4;
+        };
+        int4 dsc[kDescPerLane];
+        int nlong = 0;  // rows of this lane with more than three predecessors
+#pragma unroll
+        for (int c = 0; c < kDescPerLane; ++c) {
+            const int i = c * 32 + lane;
+            dsc[c] = i < ndp ? scan_in_edges(order[i]) : make_int4(0, 0, 0, 0);
+            nlong += dsc[c].w > 3 ? 1 : 0;
+        }
+        for (int i = 32 * kDescPerLane + lane; i < ndp; i += 32) {
+            const int4 r4 = scan_in_edges(order[i]);
+            g.rowdesc[i] = r4;
+            nlong += r4.w > 3 ? 1 : 0;
+        }
+        __syncwarp();
+        // final descriptors: rows with more than three predecessors keep the
+        // full list in pred_idx (offsets by a warp prefix over their counts)
+        const bool any_long = __any_sync(0xffffffffu, nlong > 0);
+        int list_base = 0;
+        auto finish = [&](int i, int4 dd) {
+            const int v = i < ndp ? order[i] : 0;
+            int off = 0;
+            if (any_long) {
+                int tot = 0;
+                const int cntl = (i < ndp && dd.w > 3) ? dd.w : 0;
+                off = list_base + warp_excl(cntl, lane, tot);
+                list_base += tot;
+                if (cntl) {
+                    int k = off;
+                    for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e]) {
+                        const int r = dpr[g.e_src[e]] & 0x7FFFFFFF;
+                        if (r > 0) g.pred_idx[k++] = r;
+                    }
+                }
+            }
+            if (i < ndp) {
+                const bool sink = (dpr[v] & 0x80000000) == 0;
+                g.sink[i] = sink ? 1 : 0;
+                g.rowdesc[i] = make_int4(dd.w > 3 ? off : dd.x, dd.y, dd.z,
+                                         int(uint32_t(dd.w) | (uint32_t(sink) << 17) | (uint32_t(g.code[v]) << 24)));
+            }
+        };
+#pragma unroll
+        for (int c = 0; c < kDescPerLane; ++c)
+            if (c * 32 < ndp) finish(c * 32 + lane, dsc[c]);
+        for (int c0 = 32 * kDescPerLane; c0 < ndp; c0 += 32) {
+            const int i = c0 + lane;
+            finish(i, i < ndp ? g.rowdesc[i] : make_int4(0, 0, 0, 0));
         }
         __syncwarp();
         const EndCell ec = dp_dispatch(a, g, order, ndp, seq, L, lane, ring);
