@@ -48,7 +48,7 @@ def _args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    p.add_argument("--config", type=int, default=1, choices=[0, 1, 4])
+    p.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3, 4])
     p.add_argument("--scale", type=float, default=1.0, help="genome scale (1.0 = the named workload)")
     p.add_argument("--cpu-sample", type=int, default=400, help="windows in the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -56,6 +56,7 @@ def _args():
     p.add_argument("--serving-jobs", type=int, default=12, help="config-4 jobs in the serving measurement "
                    "(0 = skip it)")
     p.add_argument("--workers", type=int, default=4, help="serving-loop workers")
+    p.add_argument("--pairs", type=int, default=10000, help="config-2 pairs per step")
     return p.parse_args()
 
 
@@ -124,12 +125,37 @@ def _dist():
     return world, rank, local
 
 
+def max_over_ranks(seconds, world):
+    """The largest of every rank's seconds (all ranks call it in the same
+    order). The tensor lives where the process group's backend wants it: the
+    current CUDA device under NCCL, host memory under gloo."""
+    if world <= 1:
+        return float(seconds)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard_seed(config, rank):
+    """Each rank polishes its own job (weak scaling): seed = config + 1000 * rank."""
+    return config + 1000 * rank
+
+
 def _data(args, rank):
     from racon_b200 import synthetic
     base = args.data_dir or os.path.join(tempfile.gettempdir(), "racon_b200_bench")
     d = os.path.join(base, "config%d_scale%g_rank%d" % (args.config, args.scale, rank))
-    seed = args.config + 1000 * rank
+    seed = shard_seed(args.config, rank)
     marker = os.path.join(d, "done")
+    if args.config == 3:
+        if not os.path.exists(marker):
+            r, o, t, info = synthetic.fragment(d, **_fragment_shape(args.scale), seed=seed)
+            with open(marker, "w") as fh:
+                json.dump(info, fh)
+        return os.path.join(d, "reads.fastq"), os.path.join(d, "overlaps.paf"), os.path.join(d, "reads.fastq")
     if not os.path.exists(marker):
         r, o, t, info = synthetic.contig(d, args.config, seed=seed, scale=args.scale)
         with open(marker, "w") as fh:
@@ -138,7 +164,19 @@ def _data(args, rank):
     return os.path.join(d, "reads." + ext), os.path.join(d, "overlaps.paf"), os.path.join(d, "draft.fasta")
 
 
+def _fragment_shape(scale):
+    """Config 3: 5 Mb truth in 3 contigs, local depth a sinusoid in 10-200x,
+    log-normal reads (mean 10 kb), 15% error, Phred U[3,40]; scaled genome."""
+    return dict(genome=max(30_000, int(5_000_000 * scale)), contigs=3, depth=(10, 200), mean=10_000, sd=4_000,
+                err=0.15, qual_range=(3, 40))
+
+
 def _workload(args):
+    if args.config == 3:
+        return {"workload": "window POA consensus, config 3 fragment correction (-f): %d bp genome in 3 contigs "
+                            "(5 Mb x scale), depth 10-200x sinusoid, 15%% error FASTQ, all-vs-all dual PAF, "
+                            "-w 500 -m 3 -x -5 -g -4" % _fragment_shape(args.scale)["genome"],
+                "genome_scale": args.scale, "l2": "flushed between steps (512 MiB write); per-step scratch > L2"}
     return {"workload": "window POA consensus, config %d (%s)" % (args.config, {
         1: "1 Mb genome, 50x FASTQ 12% error, PAF +-50 bp, -w 500 -m 3 -x -5 -g -4",
         0: "50 kb genome, 30x FASTA 13% error, PAF, -w 500 -m 3 -x -5 -g -4"}[args.config]),
@@ -238,11 +276,132 @@ def run_serving(args, device, rates):
     return out
 
 
+def _oracle_align(pairs, threads):
+    """CPU oracle (edlib NW + path restatement) over pairs on `threads`
+    threads (the ctypes call releases the GIL); returns seconds."""
+    import concurrent.futures
+    import oracle
+    oracle.load()
+    t0 = time.perf_counter()
+    with concurrent.futures.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda p: oracle.nw_cigar(p["query"], p["target"]), pairs))
+    return time.perf_counter() - t0
+
+
+def _align_workload(args):
+    return {"workload": "overlap alignment batch, config 2 shape: %d pairs per step (the named batch is 100k), "
+                        "target spans U[1 kb, 50 kb], query = span at 7%% sub + 4%% ins + 4%% del, edlib NW + "
+                        "path, CIGAR + breakpoints every 500 bp" % args.pairs,
+            "l2": "flushed between steps (512 MiB write); codes + scratch > L2"}
+
+
+def run_align(args, local, world, rank):
+    """Config 2: device overlap alignment (edit distance, CIGAR, breakpoints)."""
+    import torch
+    import racon_b200
+    from racon_b200 import synthetic
+    pairs = synthetic.pairs(args.pairs, 1_000, 50_000, seed=shard_seed(2, rank))
+    nominal = sum(len(p["query"]) * len(p["target"]) for p in pairs)
+    ctx = racon_b200.Context(local)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    ctx.align_stage(pairs, want_cigar=True)
+    for _ in range(args.warmup):
+        ctx.align_run()
+    ref = ctx.align_fetch()
+    clocks = Clocks(local)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks.start()
+    kms, launches = [], 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ctx.align_run()
+        st = ctx.align_stats()
+        kms.append(st.kernel_ms)
+        launches += st.launches
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    assert ctx.align_fetch() == ref, "device results changed between steps"
+    dev_s = sum(kms) / 1000.0
+    t_max = max_over_ranks(dev_s, world)
+    dev_s_max = t_max
+    value = world * len(pairs) * args.steps / dev_s_max
+    # end to end: rb_align_batch with host buffers
+    ctx.align(pairs, want_cigar=True)
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        res = ctx.align(pairs, want_cigar=True)
+        st = ctx.align_stats()
+        h2d += st.h2d_bytes
+        d2h += st.d2h_bytes
+    e2e_s = time.perf_counter() - t0
+    assert res == ref
+    # roofline: minimal Myers band of the final distance, ~34 int32 ops per
+    # 64-row word and column
+    words = 0
+    for p, r in zip(pairs, ref):
+        m, n, d = len(p["query"]), len(p["target"]), r["edit_distance"]
+        words += n * -(-(2 * d + abs(m - n) + 1) // 64)
+    peaks, _ = _peaks()
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    int_peak_tops = sm_count * 128 * sm_mhz * 1e6 / 1e12
+    achieved_tops = words * 34 * args.steps / dev_s / 1e12
+    in_bytes = sum(len(p["query"]) + len(p["target"]) for p in pairs)
+    out_bytes = sum(len(r["cigar"]) + 8 * len(r["breakpoints"]) + 4 for r in ref)
+    achieved_gbs = (in_bytes + out_bytes) * args.steps / dev_s / 1e9
+    out = {"metric": "overlap alignment pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dev_s_max / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 bit-vectors",
+           "data": "synthetic (seeded)", "config": _align_workload(args),
+           "gcups_nominal": nominal * args.steps / dev_s / 1e9, "gpu_launches": launches,
+           "e2e": {"value": world * len(pairs) * args.steps / e2e_s, "unit": "pairs/s",
+                   "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
+           "roofline": {"bound": "hbm", "kernel": "nw_distance_kernel + nw_level_kernel",
+                        "achieved": achieved_gbs, "peak": peaks.get("hbm_gbs", 6650.0), "unit": "GB/s",
+                        "frac": achieved_gbs / peaks.get("hbm_gbs", 6650.0), "traffic": None,
+                        "note": "algorithmic bytes = sequences in + CIGAR and breakpoints out; the sweep is "
+                                "integer-issue bound, see compute"},
+           "compute": {"bound": "int32 issue", "achieved_tops": achieved_tops, "peak_tops": int_peak_tops,
+                       "frac": achieved_tops / int_peak_tops, "band_words": words,
+                       "note": "minimal band of the final distance x 34 int32 ops per 64-row word"},
+           "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = pairs[:256]
+        threads = os.cpu_count() or 1
+        sec = _oracle_align(sample, threads)
+        out["cpu_baseline"] = {"value": len(sample) / sec, "unit": "pairs/s", "cores": threads, "kind": "port",
+                               "sample": "first %d of %d pairs, NW + path + CIGAR (CPU oracle)" % (len(sample),
+                                                                                              len(pairs))}
+    ctx.close()
+    return out
+
+
 def run_reference(args):
     world, rank, local = _dist()
     if rank != 0:
         return
     import oracle
+    if args.config == 2:
+        from racon_b200 import synthetic
+        pairs = synthetic.pairs(min(args.pairs, 1024), 1_000, 50_000, seed=2)
+        threads = os.cpu_count() or 1
+        _oracle_align(pairs[:4], threads)
+        secs = [_oracle_align(pairs, threads) for _ in range(args.steps)]
+        value = len(pairs) * args.steps / sum(secs)
+        print(json.dumps({"metric": "overlap alignment pairs/s", "value": value, "unit": "pairs/s",
+                          "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": 1,
+                          "ms_per_step": 1000 * sum(secs) / args.steps, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "u64 bit-vectors",
+                          "data": "synthetic (seeded)", "config": _align_workload(args),
+                          "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": threads, "kind": "port",
+                                           "sample": "first %d pairs of the batch per step (CPU oracle)" % len(pairs)},
+                          "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
     if args.config == 4:
         # the CPU oracle polishes the config-4 jobs one after another (a bounded sample of the stream)
         jobs = _serving_jobs(args)
@@ -267,7 +426,7 @@ def run_reference(args):
                                   "d2h_bytes_per_step": 0}}))
         return
     paths = _data(args, 0)
-    wins = oracle.dump_windows(*paths, threads=os.cpu_count() or 1)
+    wins = oracle.dump_windows(*paths, fragment=args.config == 3, threads=os.cpu_count() or 1)
     n_sample = min(args.cpu_sample, len(wins))
     blob = oracle.windows_blob(wins[:n_sample])
     threads = os.cpu_count() or 1
@@ -299,6 +458,17 @@ def main():
     import racon_b200
     world, rank, local = _dist()
     torch.cuda.set_device(local)
+    if args.config == 2:
+        if world > 1:
+            import datetime
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                                 device_id=torch.device("cuda", local))
+        out = run_align(args, local, world, rank)
+        if rank == 0:
+            print(json.dumps(out))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if args.config == 4:
         # serving loop alone: load sweep over the config-4 job stream
         res = run_serving(args, local, [0.25, 0.5, 0.8, 1.0])
@@ -319,7 +489,8 @@ def main():
                                              device_id=torch.device("cuda", local))
     m, x, g, w = 3, -5, -4, 500
     paths = _data(args, rank)
-    job = racon_b200.Job(*paths, window_length=w, match=m, mismatch=x, gap=g, device=local)
+    job = racon_b200.Job(*paths, fragment=args.config == 3, window_length=w, match=m, mismatch=x, gap=g,
+                         device=local)
     n_win, n_layers, layer_bases, bb_bases = job.layer_stats()
     ctx = racon_b200.Context(local, m, x, g, w)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
@@ -350,10 +521,8 @@ def main():
     clk = clocks.stop()
     assert ctx.poa_fetch() == reference_out, "device results changed between steps"
     dev_s = sum(kms) / 1000.0
-    t = torch.tensor([dev_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    dev_s_max = float(t.item())
+    t_max = max_over_ranks(dev_s, world)
+    dev_s_max = t_max
     value = world * n_win * args.steps / dev_s_max
     gcups = cells / dev_s / 1e9
 
@@ -370,10 +539,8 @@ def main():
         plain_launches += st.launches
     barrier()
     assert ctx.poa_fetch() == reference_out, "plain form results differ from the batched form"
-    t = torch.tensor([sum(plain_ms) / 1000.0], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    plain_value = world * n_win * args.steps / float(t.item())
+    t_max = max_over_ranks(sum(plain_ms) / 1000.0, world)
+    plain_value = world * n_win * args.steps / t_max
 
     # ---- end to end through the C ABI with host buffers ----
     for _ in range(1):
@@ -388,10 +555,8 @@ def main():
         d2h += st.d2h_bytes
     barrier()
     e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * n_win * args.steps / float(t.item())
+    t_max = max_over_ranks(e2e_s, world)
+    e2e_value = world * n_win * args.steps / t_max
     assert res == reference_out
 
     # ---- roofline of the dominant kernel (poa_kernel) ----
