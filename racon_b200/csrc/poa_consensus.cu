@@ -169,7 +169,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(N * 4, 29);       // bpred
     take(N * 4, 30);       // cons
     take((N + 1) * L * 4, 31);  // H
-    take(((N + 8) & ~size_t(7)) * L, 32);  // dec, 8-row tiles
+    take(std::max(((N + 8) & ~size_t(7)) * L, (N + 1) * 256), 32);  // dec: bytes, or 32 uint2 per row
     take(N * 4, 33);       // ord
     take(N * 4, 34);       // ord2
     take(N * 4, 35);       // my_rank
@@ -886,11 +886,17 @@ constexpr int kRingDescOffset = (kRingBytesPerWarp - 512) / 16;
 // comes by shuffle), so rows are served without any cross-lane memory
 // ordering: the last R rows sit in a shared-memory ring laid out
 // [row][S/4][lane] (conflict-free int4), older rows come from global memory.
-// The next row's metadata (node, code, predecessor range, first predecessor,
-// sink flag) is loaded one row ahead. Per cell the pass keeps only T (best
-// diagonal/vertical value) and two packed decision bytes; the final values
-// are h_k = max(T_k, h_{k-1} + g) from the warp-scanned carry, and the cell
-// is horizontal exactly when h_{k-1} + g > T_k.
+// Row descriptors are prefetched 32 rows at a time.
+// Per cell: T = max over predecessors of the diagonal (H[p][j-1] + s) and
+// vertical (H[p][j] + g) terms, with the DPX forms max(a + b, c) and
+// max-with-predicate doing the add/max pairs; the horizontal term is a
+// max-plus scan (in-lane prefix as 4 independent sub-chains, warp scan of the
+// lane aggregates, one fix-up per cell). Decisions are two bit-planes per lane
+// and row (one uint2): bit k of .x = horizontal (h > T), bit k of .y = the
+// diagonal through predecessor 0 gives T (spoa tests it first). The walk
+// reads the rest from the row's predecessor count: a single predecessor
+// makes every other cell vertical through it; with several it decides again
+// from H. Requires match >= mismatch and match - mismatch <= 255.
 template <int S>
 __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* order, int ndp, const uint8_t* seq, int L,
                              int lane, int4* ring) {
@@ -901,9 +907,10 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
     static_assert(R >= 2, "ring");
     const int lc = g.lcap;
     int* const Hm = g.H;
-    uint8_t* const Dm = g.dec;
+    uint2* const D2 = reinterpret_cast<uint2*>(g.dec);
     const int* const pred_idx = g.pred_idx;
-    const int gap = a.gap, mt = a.match, mm = a.mismatch;
+    const int gap = a.gap, mm = a.mismatch;
+    const uint32_t diff4 = uint32_t(a.match - a.mismatch) * 0x01010101u;
     const int j0 = lane * S;
     uint32_t sc[Q];
 #pragma unroll
@@ -921,8 +928,6 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
     for (int k = 0; k < S; ++k) Hm[j0 + k] = (j0 + k) * gap;
     const int lane_l = L / S, k_l = L % S;
     int best_v = kNegInf, best_r = INT_MAX, ties = 0;
-    // row descriptors: one coalesced load per 32 rows, one block ahead,
-    // served from a 32-entry shared block
     int4* const dblk = ring + kRingDescOffset;
     const int4* const rowdesc = g.rowdesc;
     int4 pre = lane < ndp ? rowdesc[lane] : make_int4(0, 0, 0, 0);
@@ -940,12 +945,12 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         const bool is_sink = desc_sink(d.w);
         const uint32_t cmask = desc_base(d.w) * 0x01010101u;
         const int p0 = np > 3 ? pred_idx[d.x] : d.x;
-        uint32_t eq[Q];
+        // per cell: match - mismatch where the base matches, else 0 (bytes)
+        uint32_t sw[Q];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) eq[q] = __vcmpeq4(sc[q], cmask);
+        for (int q = 0; q < Q; ++q) sw[q] = __vcmpeq4(sc[q], cmask) & diff4;
         int T[S];
         int hv[S];
-        // bit k: the diagonal through predecessor 0 gives T_k (spoa tests it first)
         uint32_t dbit = 0;
         auto load_row = [&](int r) {
             if (r == 0) {
@@ -966,6 +971,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
                 }
             }
         };
+        auto sbyte = [&](int k) -> int { return int((sw[k >> 2] >> (8 * (k & 3))) & 0xFFu); };
         load_row(np == 0 ? 0 : p0);
         {
             int left = __shfl_up_sync(kFull, hv[S - 1], 1);
@@ -973,76 +979,59 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 const int pv = k == 0 ? left : hv[k - 1];
-                const bool same = (eq[k / 4] >> (8 * (k % 4))) & 1u;
-                const int dg = pv + (same ? mt : mm);
-                const int vt = hv[k] + gap;
-                T[k] = max(dg, vt);
-                dbit |= uint32_t(dg >= vt) << k;
+                const int dg = pv + mm + sbyte(k);
+                bool dge;
+                T[k] = __vibmax_s32(dg, hv[k] + gap, &dge);
+                dbit |= uint32_t(dge) << k;
             }
         }
-        uint32_t vbit = ~0u;  // single predecessor: non-diagonal cells are vertical through it
         for (int p = 1; p < np; ++p) {
             load_row(np > 3 ? pred_idx[d.x + p] : (p == 1 ? d.y : d.z));
             int left = __shfl_up_sync(kFull, hv[S - 1], 1);
             if (lane == 0) left = kNegInf;
-            vbit = 0u;  // several predecessors: the walk decides the rest from H
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 const int pv = k == 0 ? left : hv[k - 1];
-                const bool same = (eq[k / 4] >> (8 * (k % 4))) & 1u;
-                const int mx = max(pv + (same ? mt : mm), hv[k] + gap);
-                dbit &= ~(uint32_t(mx > T[k]) << k);
-                T[k] = max(T[k], mx);
+                const int mx = __viaddmax_s32(hv[k], gap, pv + mm + sbyte(k));
+                bool keep;
+                T[k] = __vibmax_s32(T[k], mx, &keep);
+                dbit &= ~(uint32_t(!keep) << k);
             }
         }
-        // horizontal term: in-lane prefix as 4 independent sub-chains, warp
-        // scan of the lane aggregates, then every cell from its sub-chain's
-        // carry-in
+        // horizontal term
         constexpr int C = S / 4;  // cells per sub-chain
         int agg[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            int run = kNegInf;
+            int run = T[c * C];
+            hv[c * C] = run;
 #pragma unroll
-            for (int k = c * C; k < (c + 1) * C; ++k) {
-                run = max(T[k], run + gap);
+            for (int k = c * C + 1; k < (c + 1) * C; ++k) {
+                run = __viaddmax_s32(run, gap, T[k]);
                 hv[k] = run;
             }
             agg[c] = run;
         }
         int x = agg[0];
 #pragma unroll
-        for (int c = 1; c < 4; ++c) x = max(agg[c], x + C * gap);
+        for (int c = 1; c < 4; ++c) x = __viaddmax_s32(x, C * gap, agg[c]);
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(kFull, x, o);
-            if (lane >= o) x = max(x, y + o * S * gap);
+            if (lane >= o) x = __viaddmax_s32(y, o * S * gap, x);
         }
         int cin = __shfl_up_sync(kFull, x, 1);  // final value left of the segment
         if (lane == 0) cin = kNegInf;
-        const int carry = cin;
+        uint32_t hbit = 0;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const int next = max(agg[c], cin + C * gap);
+            const int next = __viaddmax_s32(cin, C * gap, agg[c]);
 #pragma unroll
-            for (int k = c * C; k < (c + 1) * C; ++k) hv[k] = max(hv[k], cin + (k - c * C + 1) * gap);
-            cin = next;
-        }
-        uint32_t dec4[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) dec4[q] = 0;
-#pragma unroll
-        for (int k = 0; k < S; ++k) {
-            const int hl = (k == 0 ? carry : hv[k - 1]) + gap;
-            uint32_t dd;
-            if (hl > T[k]) {
-                dd = 128u;
-            } else if ((dbit >> k) & 1u) {
-                dd = 0u;
-            } else {
-                dd = (vbit >> k) & 1u ? 64u : 255u;
+            for (int k = c * C; k < (c + 1) * C; ++k) {
+                hv[k] = __viaddmax_s32(cin, (k - c * C + 1) * gap, hv[k]);
+                hbit |= uint32_t(hv[k] > T[k]) << k;
             }
-            dec4[k / 4] |= dd << (8 * (k % 4));
+            cin = next;
         }
         int4* dst_g = reinterpret_cast<int4*>(Hm + i * lc + j0);
         int4* dst_r = ring + (i % R) * Q * 32 + lane;
@@ -1052,8 +1041,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
             dst_g[q] = v4;
             dst_r[q * 32] = v4;
         }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) *reinterpret_cast<uint32_t*>(Dm + dec_at(i, j0 + 4 * q, lc)) = dec4[q];
+        D2[i * 32 + lane] = make_uint2(hbit, dbit);
         if (lane == lane_l && is_sink) {
             int val = kNegInf;
 #pragma unroll
@@ -1073,9 +1061,14 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
                    __shfl_sync(kFull, ties, lane_l)};
 }
 
+// True when the layer's DP runs in dp_layer_fast (bit-plane decisions).
+__device__ __forceinline__ bool fast_dp(const PoaArgs& a, int L) {
+    return L + 1 <= 32 * 24 && a.match >= a.mismatch && a.match - a.mismatch <= 255;
+}
+
 __device__ EndCell dp_dispatch(const PoaArgs& a, const Graph& g, const int* order, int ndp, const uint8_t* seq, int L,
                            int lane, int4* ring) {
-    if (L + 1 <= 32 * 24) {
+    if (fast_dp(a, L)) {
         switch (seg_cells(L + 1)) {
             case 4: return dp_layer_fast<4>(a, g, order, ndp, seq, L, lane, ring);
             case 8: return dp_layer_fast<8>(a, g, order, ndp, seq, L, lane, ring);
@@ -1097,6 +1090,8 @@ __device__ EndCell dp_dispatch(const PoaArgs& a, const Graph& g, const int* orde
 __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const int* order, const uint8_t* seq,
                           int L, int iend) {
     const int lc = g.lcap;
+    const bool bits = fast_dp(a, L);
+    const int S = seg_cells(L + 1);
     int i = iend, j = L, n = 0;
     if (iend == INT_MAX || iend < 1) return false;
     while (!(i == 0 && j == 0)) {
@@ -1110,8 +1105,16 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
         }
         const int4 d = g.rowdesc[i - 1];
         const int v = order[i - 1];
-        uint32_t code = g.dec[dec_at(i, j, lc)];
         const int np = desc_np(d.w);
+        uint32_t code;
+        if (bits) {
+            // bit-plane decisions of dp_layer_fast
+            const uint2 w = reinterpret_cast<const uint2*>(g.dec)[i * 32 + j / S];
+            const int k = j % S;
+            code = (w.x >> k) & 1u ? 128u : (w.y >> k) & 1u ? 0u : np <= 1 ? 64u : 255u;
+        } else {
+            code = g.dec[dec_at(i, j, lc)];
+        }
         if (code == 255u) {  // predecessor index >= 63: decide again from H
             const int h = g.H[i * lc + j];
             const int s = j > 0 ? (uint32_t(seq[j - 1]) == desc_base(d.w) ? a.match : a.mismatch) : 0;
@@ -1429,8 +1432,10 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
 }
 
 constexpr int kWarpsPerCta = 4;
+// resident CTAs per SM the register budget is sized for
+constexpr int kCtasPerSm = 3;
 
-__global__ void __launch_bounds__(32 * kWarpsPerCta, 3) poa_kernel(PoaArgs a) {
+__global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) poa_kernel(PoaArgs a) {
     __shared__ PoaShared sh_all[kWarpsPerCta];
     // the per-warp view of its scratch slot lives in shared memory so the
     // ~35 array pointers are not held in registers across the DP
@@ -1455,7 +1460,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, 3) poa_kernel(PoaArgs a) {
 // Plain comparison form: one window per one-warp block, block b takes window
 // order[b] with scratch slot b, one launch per batch, no work queue. Same
 // per-window code as poa_kernel, so results are identical.
-__global__ void __launch_bounds__(32 * kWarpsPerCta, 3) poa_plain_kernel(PoaArgs a) {
+__global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) poa_plain_kernel(PoaArgs a) {
     __shared__ PoaShared sh;
     __shared__ Graph g;
     extern __shared__ int4 ring_all[];
@@ -1647,7 +1652,7 @@ void PoaEngine::run(bool plain) {
         // resident windows (one warp each): enough to fill the SMs, bounded by
         // a scratch budget
         const size_t budget = scratch_budget_;
-        size_t slots = std::min<size_t>(todo.size(), plain ? todo.size() : size_t(dev_.sm_count) * 12);
+        size_t slots = std::min<size_t>(todo.size(), plain ? todo.size() : size_t(dev_.sm_count) * kWarpsPerCta * kCtasPerSm);
         // RB_POA_SLOTS caps the resident windows (smaller scratch, e.g. for
         // profiler captures); results do not depend on it
         if (const char* e = getenv("RB_POA_SLOTS"))
