@@ -137,6 +137,8 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     };
     const size_t N = size_t(ncap), E = size_t(ecap), A = size_t(acap), L = size_t(lcap);
     const size_t S = N + E + A + 16;
+    // graph arrays (touched by the pointer-walking steps) first, packed;
+    // the DP matrices, streamed once per layer, last
     take(N, 0);            // code
     take(N * 4, 1);        // cov
     take(N * 4, 2);        // in_head
@@ -160,16 +162,6 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(E * 4, 20);       // e_next_out
     take(A * 4, 21);       // a_node
     take(A * 4, 22);       // a_next
-    take(S * 4, 23);       // stack
-    take((N + 2) * 4, 24); // pred_off
-    take((E + N + 2) * 4, 25);  // pred_idx
-    take((N + L + 2) * 4, 26);  // aln_node
-    take((N + L + 2) * 4, 27);  // aln_pos
-    take(N * 8, 28);       // bscore
-    take(N * 4, 29);       // bpred
-    take(N * 4, 30);       // cons
-    take((N + 1) * L * 4, 31);  // H
-    take(std::max(((N + 8) & ~size_t(7)) * L, (N + 1) * 256), 32);  // dec: bytes, or 32 uint2 per row
     take(N * 4, 33);       // ord
     take(N * 4, 34);       // ord2
     take(N * 4, 35);       // my_rank
@@ -177,6 +169,18 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(N * 4, 37);       // nw_node
     take(N * 4, 38);       // nw_slot
     take((N + 32) * 16, 39);  // rowdesc
+    take((N + 2) * 4, 24); // pred_off
+    take((E + N + 2) * 4, 25);  // pred_idx
+    take((N + L + 2) * 4, 26);  // aln_node
+    take((N + L + 2) * 4, 27);  // aln_pos
+    take(N * 8, 28);       // bscore
+    take(N * 4, 29);       // bpred
+    take(N * 4, 30);       // cons
+    take(S * 4, 23);       // stack
+    take((N + 1) * L * 4, 31);  // H
+    take(std::max(((N + 8) & ~size_t(7)) * L, (N + 1) * 256), 32);  // dec: bytes, or 32 uint2 per row
+    // whole 2 MiB pages per slot, so that a slot's graph arrays share one page
+    off = (off + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
     return off;
 }
 
@@ -876,8 +880,6 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
 constexpr int kRingBytesPerWarp = 16384;
 // node ranks held in the ring's shared memory during the descriptor build
 constexpr int kSmemRanks = (kRingBytesPerWarp - 512) / 4;
-// row descriptors a lane keeps in registers between the two build passes
-constexpr int kDescPerLane = 4;
 // last 512 bytes of each warp's ring hold the 32-row descriptor block
 constexpr int kRingDescOffset = (kRingBytesPerWarp - 512) / 16;
 
@@ -1038,10 +1040,10 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int4 v4 = make_int4(hv[4 * q], hv[4 * q + 1], hv[4 * q + 2], hv[4 * q + 3]);
-            dst_g[q] = v4;
+            __stcs(dst_g + q, v4);  // streamed: keep the graph arrays in L2
             dst_r[q * 32] = v4;
         }
-        D2[i * 32 + lane] = make_uint2(hbit, dbit);
+        __stcs(D2 + i * 32 + lane, make_uint2(hbit, dbit));
         if (lane == lane_l && is_sink) {
             int val = kNegInf;
 #pragma unroll
@@ -1256,44 +1258,54 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         __syncwarp();
         for (int i = lane; i < ndp; i += 32) dpr[order[i]] = i + 1;
         __syncwarp();
-        // one pass over each row's in-edges (in-edge order = spoa's order):
-        // the first three predecessor ranks and the count, and the successor
-        // mark on every predecessor. The first 32 * kDescPerLane rows keep
-        // their partial descriptor in registers, the rest in global scratch.
-        auto scan_in_edges = [&](int v) {
-            int4 r4 = make_int4(0, 0, 0, 0);
-            for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e]) {
-                const int src = g.e_src[e];
-                const int r = dpr[src] & 0x7FFFFFFF;
-                if (r > 0) {
-                    if (r4.w == 0) r4.x = r;
-                    else if (r4.w == 1) r4.y = r;
-                    else if (r4.w == 2) r4.z = r;
-                    ++r4.w;
-                    atomicOr(reinterpret_cast<unsigned*>(&dpr[src]), 0x80000000u);
+        // Predecessors by one pass over the edges in id order. A node's
+        // in-edge list is in edge-id order (each layer adds at most one edge
+        // into a node, with a fresh, larger id), which is spoa's predecessor
+        // order. Lanes take 32 consecutive edges; edges into the same row
+        // are ranked by lane, so the order is deterministic. rowdesc[r - 1]
+        // collects the first three predecessor ranks (x, y, z) and the count
+        // (w) of row r; bit 31 of dpr marks a node with a successor row.
+        for (int i = lane; i < ndp; i += 32) g.rowdesc[i] = make_int4(0, 0, 0, 0);
+        __syncwarp();
+        const int E = sh.nedges;
+        const unsigned below = (1u << lane) - 1u;
+        bool any_long = false;
+        for (int c0 = 0; c0 < E; c0 += 32) {
+            const int e = c0 + lane;
+            int rs = 0, rd = 0, src = 0;
+            if (e < E) {
+                src = g.e_src[e];
+                const int dst = g.e_dst[e];
+                rs = dpr[src] & 0x7FFFFFFF;
+                rd = rs > 0 ? dpr[dst] & 0x7FFFFFFF : 0;
+            }
+            const bool q = rs > 0 && rd > 0;
+            const unsigned grp = __match_any_sync(0xffffffffu, q ? rd : -1 - lane);
+            int cnt = 0;
+            if (q) {
+                atomicOr(reinterpret_cast<unsigned*>(&dpr[src]), 0x80000000u);
+                cnt = g.rowdesc[rd - 1].w;
+            }
+            __syncwarp();
+            if (q) {
+                const int pos = cnt + __popc(grp & below);
+                int* rdw = reinterpret_cast<int*>(&g.rowdesc[rd - 1]);
+                if (pos < 3) rdw[pos] = rs;
+                if ((grp & below) == 0) {
+                    const int tot = cnt + __popc(grp);
+                    rdw[3] = tot;
+                    any_long |= tot > 3;
                 }
             }
-            return r4;
-        };
-        int4 dsc[kDescPerLane];
-        int nlong = 0;  // rows of this lane with more than three predecessors
-#pragma unroll
-        for (int c = 0; c < kDescPerLane; ++c) {
-            const int i = c * 32 + lane;
-            dsc[c] = i < ndp ? scan_in_edges(order[i]) : make_int4(0, 0, 0, 0);
-            nlong += dsc[c].w > 3 ? 1 : 0;
+            __syncwarp();
         }
-        for (int i = 32 * kDescPerLane + lane; i < ndp; i += 32) {
-            const int4 r4 = scan_in_edges(order[i]);
-            g.rowdesc[i] = r4;
-            nlong += r4.w > 3 ? 1 : 0;
-        }
-        __syncwarp();
-        // final descriptors: rows with more than three predecessors keep the
-        // full list in pred_idx (offsets by a warp prefix over their counts)
-        const bool any_long = __any_sync(0xffffffffu, nlong > 0);
+        any_long = __any_sync(0xffffffffu, any_long);
+        // final descriptors; rows with more than three predecessors get their
+        // full list in pred_idx at an offset from a warp prefix of the counts
         int list_base = 0;
-        auto finish = [&](int i, int4 dd) {
+        for (int c0 = 0; c0 < ndp; c0 += 32) {
+            const int i = c0 + lane;
+            int4 dd = i < ndp ? g.rowdesc[i] : make_int4(0, 0, 0, 0);
             const int v = i < ndp ? order[i] : 0;
             int off = 0;
             if (any_long) {
@@ -1301,13 +1313,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
                 const int cntl = (i < ndp && dd.w > 3) ? dd.w : 0;
                 off = list_base + warp_excl(cntl, lane, tot);
                 list_base += tot;
-                if (cntl) {
-                    int k = off;
-                    for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e]) {
-                        const int r = dpr[g.e_src[e]] & 0x7FFFFFFF;
-                        if (r > 0) g.pred_idx[k++] = r;
-                    }
-                }
+                if (cntl) g.bpred[v] = off;  // list cursor of the node
             }
             if (i < ndp) {
                 const bool sink = (dpr[v] & 0x80000000) == 0;
@@ -1315,13 +1321,32 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
                 g.rowdesc[i] = make_int4(dd.w > 3 ? off : dd.x, dd.y, dd.z,
                                          int(uint32_t(dd.w) | (uint32_t(sink) << 17) | (uint32_t(g.code[v]) << 24)));
             }
-        };
-#pragma unroll
-        for (int c = 0; c < kDescPerLane; ++c)
-            if (c * 32 < ndp) finish(c * 32 + lane, dsc[c]);
-        for (int c0 = 32 * kDescPerLane; c0 < ndp; c0 += 32) {
-            const int i = c0 + lane;
-            finish(i, i < ndp ? g.rowdesc[i] : make_int4(0, 0, 0, 0));
+        }
+        __syncwarp();
+        if (any_long) {
+            // second pass over the edges for the long lists, same ranking
+            for (int c0 = 0; c0 < E; c0 += 32) {
+                const int e = c0 + lane;
+                int rs = 0, dst = 0;
+                bool q = false;
+                if (e < E) {
+                    dst = g.e_dst[e];
+                    const int rd = dpr[dst] & 0x7FFFFFFF;
+                    if (rd > 0 && desc_np(g.rowdesc[rd - 1].w) > 3) {
+                        rs = dpr[g.e_src[e]] & 0x7FFFFFFF;
+                        q = rs > 0;
+                    }
+                }
+                const unsigned grp = __match_any_sync(0xffffffffu, q ? dst : -1 - lane);
+                int cur = 0;
+                if (q) cur = g.bpred[dst];
+                __syncwarp();
+                if (q) {
+                    g.pred_idx[cur + __popc(grp & below)] = rs;
+                    if ((grp & below) == 0) g.bpred[dst] = cur + __popc(grp);
+                }
+                __syncwarp();
+            }
         }
         __syncwarp();
         const EndCell ec = dp_dispatch(a, g, order, ndp, seq, L, lane, ring);
