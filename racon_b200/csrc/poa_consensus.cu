@@ -119,6 +119,10 @@ __device__ __forceinline__ size_t dec_at(int i, int j, int lc) {
     return size_t(i) * size_t(lc) + size_t(j);
 }
 
+// Decision bit-planes of dp_layer_fast: one uint2 per (row, lane), row-major
+// (each row is one coalesced 256-byte store).
+__device__ __forceinline__ size_t bits_at(int i, int lane) { return size_t(i) * 32u + size_t(lane); }
+
 // Row descriptor word w: predecessor count (17 bits) | sink << 17 | base << 24.
 __device__ __forceinline__ int desc_np(int w) { return w & 0x1FFFF; }
 __device__ __forceinline__ bool desc_sink(int w) { return (w >> 17) & 1; }
@@ -178,7 +182,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(N * 4, 30);       // cons
     take(S * 4, 23);       // stack
     take((N + 1) * L * 4, 31);  // H
-    take(std::max(((N + 8) & ~size_t(7)) * L, (N + 1) * 256), 32);  // dec: bytes, or 32 uint2 per row
+    take(std::max(((N + 8) & ~size_t(7)) * L, ((N + 16) & ~size_t(15)) * 256), 32);  // dec: bytes or bit-planes
     // whole 2 MiB pages per slot, so that a slot's graph arrays share one page
     off = (off + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
     return off;
@@ -1043,7 +1047,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
             __stcs(dst_g + q, v4);  // streamed: keep the graph arrays in L2
             dst_r[q * 32] = v4;
         }
-        __stcs(D2 + i * 32 + lane, make_uint2(hbit, dbit));
+        __stcs(D2 + bits_at(i, lane), make_uint2(hbit, dbit));
         if (lane == lane_l && is_sink) {
             int val = kNegInf;
 #pragma unroll
@@ -1095,6 +1099,16 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
     const bool bits = fast_dp(a, L);
     const int S = seg_cells(L + 1);
     int i = iend, j = L, n = 0;
+    int seg = L / S, k = L % S;  // column j = seg * S + k, kept in step with j
+    auto step_left = [&]() {
+        --j;
+        if (k == 0) {
+            k = S - 1;
+            --seg;
+        } else {
+            --k;
+        }
+    };
     if (iend == INT_MAX || iend < 1) return false;
     while (!(i == 0 && j == 0)) {
         if (n >= g.alncap) return false;
@@ -1102,7 +1116,7 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             g.aln_node[n] = -1;
             g.aln_pos[n] = j - 1;
             ++n;
-            --j;
+            step_left();
             continue;
         }
         const int4 d = g.rowdesc[i - 1];
@@ -1110,28 +1124,49 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
         const int np = desc_np(d.w);
         uint32_t code;
         if (bits) {
-            // bit-plane decisions of dp_layer_fast
-            const uint2 w = reinterpret_cast<const uint2*>(g.dec)[i * 32 + j / S];
-            const int k = j % S;
+            // bit-plane decisions of dp_layer_fast (segment seg, cell k of column j)
+            const uint2 w = reinterpret_cast<const uint2*>(g.dec)[bits_at(i, seg)];
             code = (w.x >> k) & 1u ? 128u : (w.y >> k) & 1u ? 0u : np <= 1 ? 64u : 255u;
         } else {
             code = g.dec[dec_at(i, j, lc)];
         }
-        if (code == 255u) {  // predecessor index >= 63: decide again from H
+        if (code == 255u) {  // decide again from H: diagonal, then vertical, preds in order
             const int h = g.H[i * lc + j];
             const int s = j > 0 ? (uint32_t(seq[j - 1]) == desc_base(d.w) ? a.match : a.mismatch) : 0;
             const int cnt = np == 0 ? 1 : np;
             code = 128u;
             int pick = -1;
-            if (j > 0)
-                for (int p = 0; p < cnt && pick < 0; ++p)
-                    if (g.H[desc_pred(g, d, p) * lc + j - 1] + s == h) pick = p;
-            if (pick >= 0) {
-                code = 1000u + uint32_t(pick);
+            if (cnt <= 3) {
+                // all candidate values loaded at once (independent loads)
+                int hd[3], hvv[3];
+#pragma unroll
+                for (int p = 0; p < 3; ++p) {
+                    const int r = p < cnt ? desc_pred(g, d, p) : 0;
+                    hd[p] = (p < cnt && j > 0) ? g.H[r * lc + j - 1] : kNegInf;
+                    hvv[p] = p < cnt ? g.H[r * lc + j] : kNegInf;
+                }
+#pragma unroll
+                for (int p = 2; p >= 0; --p)
+                    if (j > 0 && hd[p] + s == h) pick = p;
+                if (pick >= 0) {
+                    code = 1000u + uint32_t(pick);
+                } else {
+#pragma unroll
+                    for (int p = 2; p >= 0; --p)
+                        if (hvv[p] + a.gap == h) pick = p;
+                    if (pick >= 0) code = 2000u + uint32_t(pick);
+                }
             } else {
-                for (int p = 0; p < cnt && pick < 0; ++p)
-                    if (g.H[desc_pred(g, d, p) * lc + j] + a.gap == h) pick = p;
-                if (pick >= 0) code = 2000u + uint32_t(pick);
+                if (j > 0)
+                    for (int p = 0; p < cnt && pick < 0; ++p)
+                        if (g.H[desc_pred(g, d, p) * lc + j - 1] + s == h) pick = p;
+                if (pick >= 0) {
+                    code = 1000u + uint32_t(pick);
+                } else {
+                    for (int p = 0; p < cnt && pick < 0; ++p)
+                        if (g.H[desc_pred(g, d, p) * lc + j] + a.gap == h) pick = p;
+                    if (pick >= 0) code = 2000u + uint32_t(pick);
+                }
             }
         }
         if (code < 64u || (code >= 1000u && code < 2000u)) {
@@ -1140,7 +1175,7 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             g.aln_pos[n] = j - 1;
             ++n;
             i = desc_pred(g, d, p);
-            --j;
+            step_left();
         } else if (code < 128u || code >= 2000u) {
             const int p = code < 128u ? int(code - 64u) : int(code - 2000u);
             i = desc_pred(g, d, p);  // vertical: no sequence position
@@ -1149,11 +1184,149 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             g.aln_node[n] = -1;
             g.aln_pos[n] = j - 1;
             ++n;
-            --j;
+            step_left();
         }
     }
     sh.naln = n;
     return true;
+}
+
+// Escape decision from H (diagonal, then vertical, predecessors in order):
+// 1000 + p for the diagonal through predecessor p, 2000 + p for the vertical
+// one, 128 for horizontal.
+__device__ uint32_t decide_from_h(const PoaArgs& a, const Graph& g, const int4& d, const uint8_t* seq, int i, int j) {
+    const int lc = g.lcap;
+    const int np = desc_np(d.w);
+    const int h = g.H[i * lc + j];
+    const int s = j > 0 ? (uint32_t(seq[j - 1]) == desc_base(d.w) ? a.match : a.mismatch) : 0;
+    const int cnt = np == 0 ? 1 : np;
+    int pick = -1;
+    if (cnt <= 3) {
+        int hd[3], hvv[3];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+            const int r = p < cnt ? desc_pred(g, d, p) : 0;
+            hd[p] = (p < cnt && j > 0) ? g.H[r * lc + j - 1] : kNegInf;
+            hvv[p] = p < cnt ? g.H[r * lc + j] : kNegInf;
+        }
+#pragma unroll
+        for (int p = 2; p >= 0; --p)
+            if (j > 0 && hd[p] + s == h) pick = p;
+        if (pick >= 0) return 1000u + uint32_t(pick);
+#pragma unroll
+        for (int p = 2; p >= 0; --p)
+            if (hvv[p] + a.gap == h) pick = p;
+        return pick >= 0 ? 2000u + uint32_t(pick) : 128u;
+    }
+    if (j > 0)
+        for (int p = 0; p < cnt && pick < 0; ++p)
+            if (g.H[desc_pred(g, d, p) * lc + j - 1] + s == h) pick = p;
+    if (pick >= 0) return 1000u + uint32_t(pick);
+    for (int p = 0; p < cnt && pick < 0; ++p)
+        if (g.H[desc_pred(g, d, p) * lc + j] + a.gap == h) pick = p;
+    return pick >= 0 ? 2000u + uint32_t(pick) : 128u;
+}
+
+// Warp form of the walk over dp_layer_fast's bit-plane decisions. The walk is
+// a chain of dependent steps through nearby rows and columns, so the warp
+// stages a window in shared memory with one parallel load: descriptors,
+// node ids and the decision words of rows [wlo, wlo + 32) in column segments
+// wseg and wseg - 1. Every lane then runs the same walk over the window
+// (uniform control flow); lane 0 writes the alignment. A step that leaves
+// the window reloads it. Returns false on a broken walk.
+__device__ bool traceback_warp(const PoaArgs& a, const Graph& g, PoaShared& sh, const int* order, const uint8_t* seq,
+                               int L, int iend, int lane, int4* ring) {
+    const int S = seg_cells(L + 1);
+    int4* const w_desc = ring;                                         // [32]
+    int* const w_node = reinterpret_cast<int*>(ring + 32);            // [32]
+    uint2* const w_bits = reinterpret_cast<uint2*>(ring + 40);        // [2][32]
+    const uint2* const D2 = reinterpret_cast<const uint2*>(g.dec);
+    int i = iend, j = L, n = 0;
+    if (iend == INT_MAX || iend < 1) return false;
+    int seg = L / S, k = L % S;
+    int wlo = INT_MAX, wseg = -1;
+    bool ok = true;
+    while (!(i == 0 && j == 0)) {
+        if (n >= g.alncap) {
+            ok = false;
+            break;
+        }
+        if (i == 0) {
+            if (lane == 0) {
+                g.aln_node[n] = -1;
+                g.aln_pos[n] = j - 1;
+            }
+            ++n;
+            --j;
+            if (k == 0) {
+                k = S - 1;
+                --seg;
+            } else {
+                --k;
+            }
+            continue;
+        }
+        if (i < wlo || i >= wlo + 32 || seg < wseg - 1 || seg > wseg) {
+            // stage rows [i - 31, i] (clamped at 1) for segments seg, seg - 1
+            __syncwarp();
+            wlo = max(1, i - 31);
+            wseg = seg;
+            const int r = wlo + lane;
+            if (r <= i) {
+                w_desc[lane] = g.rowdesc[r - 1];
+                w_node[lane] = order[r - 1];
+                w_bits[lane] = D2[bits_at(r, seg)];
+                w_bits[32 + lane] = seg > 0 ? D2[bits_at(r, seg - 1)] : make_uint2(0, 0);
+            }
+            __syncwarp();
+        }
+        const int o = i - wlo;
+        const int4 d = w_desc[o];
+        const int v = w_node[o];
+        const uint2 w = w_bits[(seg == wseg ? 0 : 32) + o];
+        const int np = desc_np(d.w);
+        uint32_t code = (w.x >> k) & 1u ? 128u : (w.y >> k) & 1u ? 0u : np <= 1 ? 64u : 255u;
+        if (code == 255u) code = decide_from_h(a, g, d, seq, i, j);
+        if (code < 64u || (code >= 1000u && code < 2000u)) {
+            const int p = code < 64u ? int(code) : int(code - 1000u);
+            if (lane == 0) {
+                g.aln_node[n] = v;
+                g.aln_pos[n] = j - 1;
+            }
+            ++n;
+            i = desc_pred(g, d, p);
+            --j;
+            if (k == 0) {
+                k = S - 1;
+                --seg;
+            } else {
+                --k;
+            }
+        } else if (code < 128u || code >= 2000u) {
+            const int p = code < 128u ? int(code - 64u) : int(code - 2000u);
+            i = desc_pred(g, d, p);  // vertical: no sequence position
+        } else {
+            if (j == 0) {
+                ok = false;
+                break;
+            }
+            if (lane == 0) {
+                g.aln_node[n] = -1;
+                g.aln_pos[n] = j - 1;
+            }
+            ++n;
+            --j;
+            if (k == 0) {
+                k = S - 1;
+                --seg;
+            } else {
+                --k;
+            }
+        }
+    }
+    __syncwarp();
+    if (lane == 0) sh.naln = n;
+    return ok;
 }
 
 // ---------------- one window (one warp) ----------------
@@ -1379,7 +1552,11 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
             }
             iend = __shfl_sync(0xffffffffu, iend, 0);
         }
-        if (lane == 0 && !sh.fail && !traceback(a, g, sh, order, seq, L, iend)) sh.fail = kFailed;
+        if (fast_dp(a, L)) {
+            if (!sh.fail && !traceback_warp(a, g, sh, order, seq, L, iend, lane, ring) && lane == 0) sh.fail = kFailed;
+        } else if (lane == 0 && !sh.fail && !traceback(a, g, sh, order, seq, L, iend)) {
+            sh.fail = kFailed;
+        }
         __syncwarp();
         if (sh.fail) break;
         add_alignment_warp(g, sh, seq, qual, L, lane);
