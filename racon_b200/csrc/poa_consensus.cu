@@ -106,6 +106,9 @@ struct Graph {
     int *ord, *ord2, *my_rank, *shift, *nw_node, *nw_slot;
     int* H;
     uint8_t* dec;
+    // per-node in-edge and aligned-entry counts, owner node of each aligned
+    // entry (for the compact lists built in shared memory)
+    int *in_cnt, *al_cnt, *a_owner;
     int ncap, ecap, acap, scap, lcap, alncap;
 };
 
@@ -173,6 +176,9 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(N * 4, 37);       // nw_node
     take(N * 4, 38);       // nw_slot
     take((N + 32) * 16, 39);  // rowdesc
+    take(N * 4, 40);       // in_cnt
+    take(N * 4, 41);       // al_cnt
+    take(A * 4, 42);       // a_owner
     take((N + 2) * 4, 24); // pred_off
     take((E + N + 2) * 4, 25);  // pred_idx
     take((N + L + 2) * 4, 26);  // aln_node
@@ -191,7 +197,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
 __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
     uint8_t* base = a.scratch + size_t(slot) * a.slot_bytes;
     Graph g;
-    void* p[40];
+    void* p[43];
     walk_layout(a.ncap, a.ecap, a.acap, a.lcap, [&](int id, size_t off) { p[id] = base + off; });
     g.code = (uint8_t*)p[0];
     g.cov = (uint32_t*)p[1];
@@ -233,6 +239,9 @@ __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
     g.nw_node = (int*)p[37];
     g.nw_slot = (int*)p[38];
     g.rowdesc = (int4*)p[39];
+    g.in_cnt = (int*)p[40];
+    g.al_cnt = (int*)p[41];
+    g.a_owner = (int*)p[42];
     g.ncap = a.ncap;
     g.ecap = a.ecap;
     g.acap = a.acap;
@@ -491,6 +500,8 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
         g.in_head[id] = g.in_tail[id] = -1;
         g.out_head[id] = g.out_tail[id] = -1;
         g.al_head[id] = g.al_tail[id] = -1;
+        g.in_cnt[id] = 0;
+        g.al_cnt[id] = 0;
     }
     __syncwarp();
     for (int t = lane; t < m; t += 32) {
@@ -506,6 +517,8 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
         int slot = sh.naligned + e_start[t];
         auto link = [&](int v, int y) {
             g.a_node[slot] = y;
+            g.a_owner[slot] = v;
+            g.al_cnt[v] += 1;  // one group per node and layer: no other lane links v
             g.a_next[slot] = -1;
             if (g.al_tail[v] == -1) g.al_head[v] = slot;
             else g.a_next[g.al_tail[v]] = slot;
@@ -556,6 +569,7 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
                 if (g.in_tail[v] == -1) g.in_head[v] = id;
                 else g.e_next_in[g.in_tail[v]] = id;
                 g.in_tail[v] = id;
+                g.in_cnt[v] += 1;  // at most one new edge into v per layer
             }
         }
         new_edges += tot;
@@ -1191,6 +1205,181 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
     return true;
 }
 
+// ---------------- compact adjacency in shared memory ----------------
+
+// In-edge sources and aligned nodes of every node as uint16 CSR lists in a
+// warp's shared memory, in the graph's own list order (in-edges by edge id,
+// aligned entries by slot: both are append-only), plus one flag byte per
+// node. The DFS steps then read shared memory instead of chasing linked
+// lists through global memory.
+struct SmemCsr {
+    uint16_t* in_off;  // [N + 1]
+    uint16_t* al_off;  // [N + 1]
+    uint16_t* in_src;  // [E]
+    uint16_t* al_x;    // [A]
+    uint8_t* flag;     // [N]: mark (bits 0-1), primary (bit 2), member (bit 3)
+};
+
+__device__ __forceinline__ size_t csr_bytes(int N, int E, int A) {
+    return 2 * (size_t(N) + 1) * 2 + 2 * size_t(E) + 2 * size_t(A) + size_t(N);
+}
+
+// Builds the lists (warp). Returns false, building nothing, when the graph
+// does not fit in `cap` bytes or 16-bit indices.
+__device__ bool build_csr(const Graph& g, const PoaShared& sh, int lane, void* smem, int cap, SmemCsr& c) {
+    const int N = sh.nnodes, E = sh.nedges, A = sh.naligned;
+    if (N >= 65535 || E >= 65535 || A >= 65535 || csr_bytes(N, E, A) > size_t(cap)) return false;
+    uint16_t* base = reinterpret_cast<uint16_t*>(smem);
+    c.in_off = base;
+    c.al_off = base + (N + 1);
+    c.in_src = base + 2 * (N + 1);
+    c.al_x = c.in_src + E;
+    c.flag = reinterpret_cast<uint8_t*>(c.al_x + A);
+    // starts: exclusive prefix of the counts
+    int bi = 0, ba = 0;
+    for (int c0 = 0; c0 < N; c0 += 32) {
+        const int v = c0 + lane;
+        int ti = 0, ta = 0;
+        const int xi = warp_excl(v < N ? g.in_cnt[v] : 0, lane, ti);
+        const int xa = warp_excl(v < N ? g.al_cnt[v] : 0, lane, ta);
+        if (v < N) {
+            c.in_off[v] = uint16_t(bi + xi);
+            c.al_off[v] = uint16_t(ba + xa);
+        }
+        bi += ti;
+        ba += ta;
+    }
+    if (lane == 0) {
+        c.in_off[N] = uint16_t(E);
+        c.al_off[N] = uint16_t(A);
+    }
+    __syncwarp();
+    // stable fill by owner: the offsets serve as cursors and end up at the
+    // next node's start
+    const unsigned below = (1u << lane) - 1u;
+    for (int c0 = 0; c0 < E; c0 += 32) {
+        const int e = c0 + lane;
+        const int dst = e < E ? g.e_dst[e] : -1 - lane;
+        const int src = e < E ? g.e_src[e] : 0;
+        const unsigned grp = __match_any_sync(0xffffffffu, dst);
+        const int cur = e < E ? c.in_off[dst] : 0;
+        __syncwarp();
+        if (e < E) {
+            c.in_src[cur + __popc(grp & below)] = uint16_t(src);
+            if ((grp & below) == 0) c.in_off[dst] = uint16_t(cur + __popc(grp));
+        }
+        __syncwarp();
+    }
+    for (int c0 = 0; c0 < A; c0 += 32) {
+        const int x = c0 + lane;
+        const int own = x < A ? g.a_owner[x] : -1 - lane;
+        const int y = x < A ? g.a_node[x] : 0;
+        const unsigned grp = __match_any_sync(0xffffffffu, own);
+        const int cur = x < A ? c.al_off[own] : 0;
+        __syncwarp();
+        if (x < A) {
+            c.al_x[cur + __popc(grp & below)] = uint16_t(y);
+            if ((grp & below) == 0) c.al_off[own] = uint16_t(cur + __popc(grp));
+        }
+        __syncwarp();
+    }
+    // shift the cursors back to starts (off[v] = end of v - 1), top chunk first
+    for (int c0 = ((N - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
+        const int v = c0 + lane;
+        uint16_t pi = 0, pa = 0;
+        if (v < N && v > 0) {
+            pi = c.in_off[v - 1];
+            pa = c.al_off[v - 1];
+        }
+        __syncwarp();
+        if (v < N) {
+            c.in_off[v] = pi;
+            c.al_off[v] = pa;
+        }
+        __syncwarp();
+    }
+    return true;
+}
+
+// g_topo_sort over the shared-memory lists (lane 0; flags initialised by the
+// caller: mark 0, primary set, member bit for the nodes taking part).
+__device__ int g_topo_sort_csr(const Graph& g, const SmemCsr& c, int N, bool all_nodes, int* out) {
+    int nr = 0;
+    int sp = 0;
+    auto member = [&](int x) { return all_nodes || (c.flag[x] & 8); };
+    auto mark = [&](int x) { return c.flag[x] & 3; };
+    auto set_mark = [&](int x, int m) { c.flag[x] = uint8_t((c.flag[x] & ~3) | m); };
+    for (int i = 0; i < N; ++i) {
+        if (!member(i) || mark(i) != 0) continue;
+        g.stack[sp++] = i;
+        while (sp > 0) {
+            const int v = g.stack[sp - 1];
+            bool valid = true;
+            if (mark(v) != 2) {
+                for (int q = c.in_off[v], qe = c.in_off[v + 1]; q < qe; ++q) {
+                    const int u = c.in_src[q];
+                    if (!member(u)) continue;
+                    if (mark(u) != 2) {
+                        if (sp >= g.scap) return -1;
+                        g.stack[sp++] = u;
+                        valid = false;
+                    }
+                }
+                if (c.flag[v] & 4) {
+                    for (int q = c.al_off[v], qe = c.al_off[v + 1]; q < qe; ++q) {
+                        const int y = c.al_x[q];
+                        if (!member(y)) continue;
+                        if (mark(y) != 2) {
+                            if (sp >= g.scap) return -1;
+                            g.stack[sp++] = y;
+                            c.flag[y] &= uint8_t(~4);
+                            valid = false;
+                        }
+                    }
+                }
+                if (valid) {
+                    set_mark(v, 2);
+                    if (c.flag[v] & 4) {
+                        out[nr++] = v;
+                        for (int q = c.al_off[v], qe = c.al_off[v + 1]; q < qe; ++q) {
+                            const int y = c.al_x[q];
+                            if (!member(y)) continue;
+                            out[nr++] = y;
+                        }
+                    }
+                } else {
+                    set_mark(v, 1);
+                }
+            }
+            if (valid) --sp;
+        }
+    }
+    return nr;
+}
+
+// spoa's topological order of the graph (all_nodes) or of the member nodes,
+// into out; shared-memory lists when they fit in the warp's ring, else the
+// global-memory walk. Warp-collective; the count is returned on every lane
+// (-1 on stack overflow).
+__device__ int topo_sort_warp(const Graph& g, PoaShared& sh, bool all_nodes, int* out, int lane, int4* ring) {
+    const int N = sh.nnodes;
+    SmemCsr c;
+    int nr = 0;
+    if (build_csr(g, sh, lane, ring, kRingBytesPerWarp, c)) {
+        for (int i = lane; i < N; i += 32) c.flag[i] = uint8_t(4 | (all_nodes || g.member[i] ? 8 : 0));
+        __syncwarp();
+        if (lane == 0) nr = g_topo_sort_csr(g, c, N, all_nodes, out);
+    } else {
+        for (int i = lane; i < N; i += 32) {
+            g.mark[i] = 0;
+            g.prim[i] = 1;
+        }
+        __syncwarp();
+        if (lane == 0) nr = g_topo_sort(g, sh, all_nodes, out);
+    }
+    return __shfl_sync(0xffffffffu, nr, 0);
+}
+
 // Escape decision from H (diagonal, then vertical, predecessors in order):
 // 1000 + p for the diagonal through predecessor p, 2000 + p for the vertical
 // one, 128 for horizontal.
@@ -1376,6 +1565,8 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         }
         g.ord[i] = i;
         g.my_rank[i] = i;
+        g.in_cnt[i] = i > 0 ? 1 : 0;
+        g.al_cnt[i] = 0;
     }
     if (lane == 0) {
         sh.nnodes = B;
@@ -1528,29 +1719,34 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         if (ec.ties > 1) {
             // several sinks share the best last-column value: spoa takes the
             // first in its own topological order of the aligned (sub)graph
-            for (int i = lane; i < N; i += 32) {
-                g.mark[i] = 0;
-                g.prim[i] = 1;
-            }
-            __syncwarp();
-            if (lane == 0) {
-                const int nr = g_topo_sort(g, sh, full, g.rank_to_node);
-                if (nr < 0) {
-                    sh.fail = kOverflow;
-                } else {
-                    for (int r = 0; r < nr; ++r) g.node_rank[g.rank_to_node[r]] = r;
-                    int best = INT_MAX;
-                    for (int i = 1; i <= ndp; ++i) {
-                        if (!g.sink[i - 1] || g.H[i * g.lcap + L] != ec.value) continue;
-                        const int rr = g.node_rank[order[i - 1]];
-                        if (rr < best) {
-                            best = rr;
-                            iend = i;
-                        }
+            const int nr = topo_sort_warp(g, sh, full, g.rank_to_node, lane, ring);
+            if (nr < 0) {
+                if (lane == 0) sh.fail = kOverflow;
+            } else {
+                for (int r = lane; r < nr; r += 32) g.node_rank[g.rank_to_node[r]] = r;
+                __syncwarp();
+                // the tied sink of lowest rank (ranks are distinct)
+                int best = INT_MAX, bi = iend;
+                for (int i = 1 + lane; i <= ndp; i += 32) {
+                    if (!g.sink[i - 1] || g.H[i * g.lcap + L] != ec.value) continue;
+                    const int rr = g.node_rank[order[i - 1]];
+                    if (rr < best) {
+                        best = rr;
+                        bi = i;
                     }
                 }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const int ob = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ob < best) {
+                        best = ob;
+                        bi = oi;
+                    }
+                }
+                iend = bi;
             }
-            iend = __shfl_sync(0xffffffffu, iend, 0);
+            __syncwarp();
         }
         if (fast_dp(a, L)) {
             if (!sh.fail && !traceback_warp(a, g, sh, order, seq, L, iend, lane, ring) && lane == 0) sh.fail = kFailed;
@@ -1565,14 +1761,8 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
     }
     // spoa's topological order of the final graph for the consensus
     if (!sh.fail) {
-        const int N2 = sh.nnodes;
-        for (int i = lane; i < N2; i += 32) {
-            g.mark[i] = 0;
-            g.prim[i] = 1;
-        }
-        __syncwarp();
+        const int nr = topo_sort_warp(g, sh, true, g.rank_to_node, lane, ring);
         if (lane == 0) {
-            const int nr = g_topo_sort(g, sh, true, g.rank_to_node);
             if (nr < 0) sh.fail = kOverflow;
             sh.nranks = nr;
         }
