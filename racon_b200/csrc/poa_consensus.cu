@@ -1380,6 +1380,54 @@ __device__ int topo_sort_warp(const Graph& g, PoaShared& sh, bool all_nodes, int
     return __shfl_sync(0xffffffffu, nr, 0);
 }
 
+// spoa's subgraph node set (g_mark_subgraph) into g.member, over the
+// shared-memory lists when they fit. Warp-collective; false on stack
+// overflow (on every lane).
+__device__ bool mark_subgraph_warp(const Graph& g, PoaShared& sh, int begin_node, int end_node, int lane, int4* ring) {
+    const int N = sh.nnodes;
+    if (end_node < 0 || end_node >= N) {
+        if (lane == 0) sh.fail = kFailed;
+        __syncwarp();
+        return true;
+    }
+    SmemCsr c;
+    bool ok = true;
+    if (build_csr(g, sh, lane, ring, kRingBytesPerWarp, c)) {
+        for (int i = lane; i < N; i += 32) c.flag[i] = 0;
+        __syncwarp();
+        if (lane == 0) {
+            int sp = 0;
+            g.stack[sp++] = end_node;
+            while (sp > 0 && ok) {
+                const int v = g.stack[--sp];
+                if (!(c.flag[v] & 8) && v >= begin_node) {
+                    for (int q = c.in_off[v], qe = c.in_off[v + 1]; q < qe; ++q) {
+                        if (sp >= g.scap) {
+                            ok = false;
+                            break;
+                        }
+                        g.stack[sp++] = c.in_src[q];
+                    }
+                    for (int q = c.al_off[v], qe = c.al_off[v + 1]; q < qe && ok; ++q) {
+                        if (sp >= g.scap) {
+                            ok = false;
+                            break;
+                        }
+                        g.stack[sp++] = c.al_x[q];
+                    }
+                    c.flag[v] |= 8;
+                }
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < N; i += 32) g.member[i] = (c.flag[i] & 8) ? 1 : 0;
+    } else if (lane == 0) {
+        ok = g_mark_subgraph(g, sh, begin_node, end_node);
+    }
+    __syncwarp();
+    return __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+}
+
 // Escape decision from H (diagonal, then vertical, predecessors in order):
 // 1000 + p for the diagonal through predecessor p, 2000 + p for the vertical
 // one, 128 for horizontal.
@@ -1590,10 +1638,10 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
             g.member[i] = full ? 1 : 0;
         }
         __syncwarp();
-        if (lane == 0) {
-            if (!full && !g_mark_subgraph(g, sh, int(Lr.begin), int(Lr.end))) sh.fail = kOverflow;
-            if (!sh.fail && row_cover(L + 1) > g.lcap) sh.fail = kOverflow;
-        }
+        if (!full && !mark_subgraph_warp(g, sh, int(Lr.begin), int(Lr.end), lane, ring) && lane == 0)
+            sh.fail = kOverflow;
+        __syncwarp();
+        if (lane == 0 && !sh.fail && row_cover(L + 1) > g.lcap) sh.fail = kOverflow;
         __syncwarp();
         if (sh.fail) break;
         // DP rows: the incremental order, restricted to the subgraph for a
