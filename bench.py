@@ -35,10 +35,10 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per DP cell of poa_kernel, from one ncu capture of
-# config 1 at 0.1 genome scale (1.785 GB read + 30.877 GB written over
+# config 1 at 0.1 genome scale (1.783 GB read + 27.339 GB written over
 # 5.839 G cells); traffic grows with the cells, so a full launch's traffic is
 # this times its cells
-POA_DRAM_BYTES_PER_CELL = (1.784984e9 + 30.877037e9) / 5838774640
+POA_DRAM_BYTES_PER_CELL = (1.783481e9 + 27.338935e9) / 5838774640
 L2_FLUSH_BYTES = 512 << 20
 
 
