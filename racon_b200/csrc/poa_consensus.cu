@@ -188,7 +188,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(N * 4, 30);       // cons
     take(S * 4, 23);       // stack
     take((N + 1) * L * 4, 31);  // H
-    take(std::max(((N + 8) & ~size_t(7)) * L, ((N + 16) & ~size_t(15)) * 256), 32);  // dec: bytes or bit-planes
+    take(std::max(((N + 8) & ~size_t(7)) * L, (N + 1) * 256), 32);  // dec: bytes, or 32 uint2 per row
     // whole 2 MiB pages per slot, so that a slot's graph arrays share one page
     off = (off + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
     return off;
@@ -723,7 +723,7 @@ __device__ int g_heaviest_bundle(const Graph& g, PoaShared& sh) {
 __device__ __forceinline__ int desc_pred(const Graph& g, const int4& d, int p) {
     const int np = desc_np(d.w);
     if (np == 0) return 0;
-    if (np > 3) return g.pred_idx[d.x + p];
+    if (np > 3) return p == 0 ? d.y : g.pred_idx[d.x + p];
     return p == 0 ? d.x : (p == 1 ? d.y : d.z);
 }
 
@@ -964,7 +964,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         const int np = desc_np(d.w);
         const bool is_sink = desc_sink(d.w);
         const uint32_t cmask = desc_base(d.w) * 0x01010101u;
-        const int p0 = np > 3 ? pred_idx[d.x] : d.x;
+        const int p0 = np > 3 ? d.y : d.x;
         // per cell: match - mismatch where the base matches, else 0 (bytes)
         uint32_t sw[Q];
 #pragma unroll
@@ -1106,23 +1106,12 @@ __device__ EndCell dp_dispatch(const PoaArgs& a, const Graph& g, const int* orde
 // base, sequence position), end of path first; vertical steps (a graph node
 // against a gap) consume no position and add nothing to the graph. Each step
 // loads the cell's decision byte and its row's descriptor (independent
-// loads); the next row comes from the descriptor.
+// loads); the next row comes from the descriptor. Used for the byte
+// decisions of the chunked dp_layer (rows over 768 columns).
 __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const int* order, const uint8_t* seq,
                           int L, int iend) {
     const int lc = g.lcap;
-    const bool bits = fast_dp(a, L);
-    const int S = seg_cells(L + 1);
     int i = iend, j = L, n = 0;
-    int seg = L / S, k = L % S;  // column j = seg * S + k, kept in step with j
-    auto step_left = [&]() {
-        --j;
-        if (k == 0) {
-            k = S - 1;
-            --seg;
-        } else {
-            --k;
-        }
-    };
     if (iend == INT_MAX || iend < 1) return false;
     while (!(i == 0 && j == 0)) {
         if (n >= g.alncap) return false;
@@ -1130,20 +1119,13 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             g.aln_node[n] = -1;
             g.aln_pos[n] = j - 1;
             ++n;
-            step_left();
+            --j;
             continue;
         }
         const int4 d = g.rowdesc[i - 1];
         const int v = order[i - 1];
         const int np = desc_np(d.w);
-        uint32_t code;
-        if (bits) {
-            // bit-plane decisions of dp_layer_fast (segment seg, cell k of column j)
-            const uint2 w = reinterpret_cast<const uint2*>(g.dec)[bits_at(i, seg)];
-            code = (w.x >> k) & 1u ? 128u : (w.y >> k) & 1u ? 0u : np <= 1 ? 64u : 255u;
-        } else {
-            code = g.dec[dec_at(i, j, lc)];
-        }
+        uint32_t code = g.dec[dec_at(i, j, lc)];
         if (code == 255u) {  // decide again from H: diagonal, then vertical, preds in order
             const int h = g.H[i * lc + j];
             const int s = j > 0 ? (uint32_t(seq[j - 1]) == desc_base(d.w) ? a.match : a.mismatch) : 0;
@@ -1189,7 +1171,7 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             g.aln_pos[n] = j - 1;
             ++n;
             i = desc_pred(g, d, p);
-            step_left();
+            --j;
         } else if (code < 128u || code >= 2000u) {
             const int p = code < 128u ? int(code - 64u) : int(code - 2000u);
             i = desc_pred(g, d, p);  // vertical: no sequence position
@@ -1198,7 +1180,7 @@ __device__ bool traceback(const PoaArgs& a, const Graph& g, PoaShared& sh, const
             g.aln_node[n] = -1;
             g.aln_pos[n] = j - 1;
             ++n;
-            step_left();
+            --j;
         }
     }
     sh.naln = n;
@@ -1428,61 +1410,65 @@ __device__ bool mark_subgraph_warp(const Graph& g, PoaShared& sh, int begin_node
     return __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
 }
 
-// Escape decision from H (diagonal, then vertical, predecessors in order):
-// 1000 + p for the diagonal through predecessor p, 2000 + p for the vertical
-// one, 128 for horizontal.
-__device__ uint32_t decide_from_h(const PoaArgs& a, const Graph& g, const int4& d, const uint8_t* seq, int i, int j) {
+// Escape decision from H for a row of several predecessors (warp, uniform
+// arguments): the first predecessor whose diagonal gives H[i][j],
+// else the first whose vertical does, else horizontal. Returns 1000 + p,
+// 2000 + p or 128. Lanes load the candidates of 32 predecessors at a time.
+__device__ uint32_t decide_from_h(const PoaArgs& a, const Graph& g, const int4& d, const uint8_t* seq, int i, int j,
+                                  int lane) {
     const int lc = g.lcap;
     const int np = desc_np(d.w);
     const int h = g.H[i * lc + j];
     const int s = j > 0 ? (uint32_t(seq[j - 1]) == desc_base(d.w) ? a.match : a.mismatch) : 0;
     const int cnt = np == 0 ? 1 : np;
-    int pick = -1;
-    if (cnt <= 3) {
-        int hd[3], hvv[3];
-#pragma unroll
-        for (int p = 0; p < 3; ++p) {
-            const int r = p < cnt ? desc_pred(g, d, p) : 0;
-            hd[p] = (p < cnt && j > 0) ? g.H[r * lc + j - 1] : kNegInf;
-            hvv[p] = p < cnt ? g.H[r * lc + j] : kNegInf;
+    int vpick = -1;
+    for (int p0 = 0; p0 < cnt; p0 += 32) {
+        const int p = p0 + lane;
+        bool dm = false, vm = false;
+        if (p < cnt) {
+            const int r = desc_pred(g, d, p);
+            dm = j > 0 && g.H[r * lc + j - 1] + s == h;
+            vm = g.H[r * lc + j] + a.gap == h;
         }
-#pragma unroll
-        for (int p = 2; p >= 0; --p)
-            if (j > 0 && hd[p] + s == h) pick = p;
-        if (pick >= 0) return 1000u + uint32_t(pick);
-#pragma unroll
-        for (int p = 2; p >= 0; --p)
-            if (hvv[p] + a.gap == h) pick = p;
-        return pick >= 0 ? 2000u + uint32_t(pick) : 128u;
+        const unsigned bd = __ballot_sync(0xffffffffu, dm);
+        if (bd) return 1000u + uint32_t(p0 + __ffs(bd) - 1);
+        const unsigned bv = __ballot_sync(0xffffffffu, vm);
+        if (bv && vpick < 0) vpick = p0 + __ffs(bv) - 1;
     }
-    if (j > 0)
-        for (int p = 0; p < cnt && pick < 0; ++p)
-            if (g.H[desc_pred(g, d, p) * lc + j - 1] + s == h) pick = p;
-    if (pick >= 0) return 1000u + uint32_t(pick);
-    for (int p = 0; p < cnt && pick < 0; ++p)
-        if (g.H[desc_pred(g, d, p) * lc + j] + a.gap == h) pick = p;
-    return pick >= 0 ? 2000u + uint32_t(pick) : 128u;
+    return vpick >= 0 ? 2000u + uint32_t(vpick) : 128u;
 }
 
 // Warp form of the walk over dp_layer_fast's bit-plane decisions. The walk is
 // a chain of dependent steps through nearby rows and columns, so the warp
 // stages a window in shared memory with one parallel load: descriptors,
-// node ids and the decision words of rows [wlo, wlo + 32) in column segments
+// node ids and the decision words of rows [wlo, wlo + 64) in column segments
 // wseg and wseg - 1. Every lane then runs the same walk over the window
 // (uniform control flow); lane 0 writes the alignment. A step that leaves
-// the window reloads it. Returns false on a broken walk.
+// the window reloads it. Decoding: horizontal plane, else the diagonal of
+// predecessor 0; rows of one predecessor are otherwise vertical through it,
+// rows of several decide again from H. Returns false on a broken walk.
 __device__ bool traceback_warp(const PoaArgs& a, const Graph& g, PoaShared& sh, const int* order, const uint8_t* seq,
                                int L, int iend, int lane, int4* ring) {
+    constexpr int W = 64;
     const int S = seg_cells(L + 1);
-    int4* const w_desc = ring;                                         // [32]
-    int* const w_node = reinterpret_cast<int*>(ring + 32);            // [32]
-    uint2* const w_bits = reinterpret_cast<uint2*>(ring + 40);        // [2][32]
+    int4* const w_desc = ring;                                           // [W]
+    int* const w_node = reinterpret_cast<int*>(ring + W);               // [W]
+    uint2* const w_bits = reinterpret_cast<uint2*>(ring + W + W / 4);   // [2][W]
     const uint2* const D2 = reinterpret_cast<const uint2*>(g.dec);
     int i = iend, j = L, n = 0;
     if (iend == INT_MAX || iend < 1) return false;
     int seg = L / S, k = L % S;
     int wlo = INT_MAX, wseg = -1;
     bool ok = true;
+    auto step_left = [&]() {
+        --j;
+        if (k == 0) {
+            k = S - 1;
+            --seg;
+        } else {
+            --k;
+        }
+    };
     while (!(i == 0 && j == 0)) {
         if (n >= g.alncap) {
             ok = false;
@@ -1494,36 +1480,42 @@ __device__ bool traceback_warp(const PoaArgs& a, const Graph& g, PoaShared& sh, 
                 g.aln_pos[n] = j - 1;
             }
             ++n;
-            --j;
-            if (k == 0) {
-                k = S - 1;
-                --seg;
-            } else {
-                --k;
-            }
+            step_left();
             continue;
         }
-        if (i < wlo || i >= wlo + 32 || seg < wseg - 1 || seg > wseg) {
-            // stage rows [i - 31, i] (clamped at 1) for segments seg, seg - 1
+        if (i < wlo || seg < wseg - 1 || seg > wseg) {
+            // stage rows [i - 63, i] (clamped at 1) for segments seg, seg - 1
             __syncwarp();
-            wlo = max(1, i - 31);
+            wlo = max(1, i - (W - 1));
             wseg = seg;
-            const int r = wlo + lane;
-            if (r <= i) {
-                w_desc[lane] = g.rowdesc[r - 1];
-                w_node[lane] = order[r - 1];
-                w_bits[lane] = D2[bits_at(r, seg)];
-                w_bits[32 + lane] = seg > 0 ? D2[bits_at(r, seg - 1)] : make_uint2(0, 0);
+#pragma unroll
+            for (int h = 0; h < W / 32; ++h) {
+                const int o = h * 32 + lane;
+                const int r = wlo + o;
+                if (r <= i) {
+                    w_desc[o] = g.rowdesc[r - 1];
+                    w_node[o] = order[r - 1];
+                    w_bits[o] = D2[bits_at(r, seg)];
+                    w_bits[W + o] = seg > 0 ? D2[bits_at(r, seg - 1)] : make_uint2(0, 0);
+                }
             }
             __syncwarp();
         }
         const int o = i - wlo;
         const int4 d = w_desc[o];
         const int v = w_node[o];
-        const uint2 w = w_bits[(seg == wseg ? 0 : 32) + o];
+        const uint2 w = w_bits[(seg == wseg ? 0 : W) + o];
         const int np = desc_np(d.w);
-        uint32_t code = (w.x >> k) & 1u ? 128u : (w.y >> k) & 1u ? 0u : np <= 1 ? 64u : 255u;
-        if (code == 255u) code = decide_from_h(a, g, d, seq, i, j);
+        uint32_t code;
+        if ((w.x >> k) & 1u) {
+            code = 128u;
+        } else if ((w.y >> k) & 1u) {
+            code = 0u;  // diagonal through predecessor 0
+        } else if (np <= 1) {
+            code = 64u;  // vertical through the only predecessor
+        } else {
+            code = decide_from_h(a, g, d, seq, i, j, lane);
+        }
         if (code < 64u || (code >= 1000u && code < 2000u)) {
             const int p = code < 64u ? int(code) : int(code - 1000u);
             if (lane == 0) {
@@ -1532,13 +1524,7 @@ __device__ bool traceback_warp(const PoaArgs& a, const Graph& g, PoaShared& sh, 
             }
             ++n;
             i = desc_pred(g, d, p);
-            --j;
-            if (k == 0) {
-                k = S - 1;
-                --seg;
-            } else {
-                --k;
-            }
+            step_left();
         } else if (code < 128u || code >= 2000u) {
             const int p = code < 128u ? int(code - 64u) : int(code - 2000u);
             i = desc_pred(g, d, p);  // vertical: no sequence position
@@ -1552,13 +1538,7 @@ __device__ bool traceback_warp(const PoaArgs& a, const Graph& g, PoaShared& sh, 
                 g.aln_pos[n] = j - 1;
             }
             ++n;
-            --j;
-            if (k == 0) {
-                k = S - 1;
-                --seg;
-            } else {
-                --k;
-            }
+            step_left();
         }
     }
     __syncwarp();
@@ -1730,7 +1710,8 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
             if (i < ndp) {
                 const bool sink = (dpr[v] & 0x80000000) == 0;
                 g.sink[i] = sink ? 1 : 0;
-                g.rowdesc[i] = make_int4(dd.w > 3 ? off : dd.x, dd.y, dd.z,
+                // long rows: x = list offset, y = first predecessor
+                g.rowdesc[i] = make_int4(dd.w > 3 ? off : dd.x, dd.w > 3 ? dd.x : dd.y, dd.z,
                                          int(uint32_t(dd.w) | (uint32_t(sink) << 17) | (uint32_t(g.code[v]) << 24)));
             }
         }
