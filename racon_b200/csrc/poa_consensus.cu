@@ -1410,6 +1410,135 @@ __device__ bool mark_subgraph_warp(const Graph& g, PoaShared& sh, int begin_node
     return __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
 }
 
+// Row descriptors with shared-memory accumulators (the ring is free until the
+// DP): node ranks as uint16 (bit 15 marks a node with a successor row) and,
+// per row, the first three predecessor ranks and the count. Loads of graph
+// arrays are issued four 32-element chunks at a time, so one memory latency
+// covers 128 edges or rows. Same order rules as the global form below.
+// Returns false, building nothing, when the graph does not fit.
+__device__ bool descriptors_smem(const Graph& g, const PoaShared& sh, const int* order, int N, int ndp, int lane,
+                                 int4* ring) {
+    constexpr unsigned kFull = 0xffffffffu;
+    const size_t rk_bytes = size_t((N + 3) / 4) * 8;
+    if (ndp >= 32768 || sh.nseq >= 65535 || rk_bytes + size_t(8) * ndp > size_t(kRingBytesPerWarp)) return false;
+    uint16_t* const rk = reinterpret_cast<uint16_t*>(ring);
+    ushort4* const acc = reinterpret_cast<ushort4*>(reinterpret_cast<uint8_t*>(ring) + rk_bytes);
+    for (int i = lane; i < N; i += 32) rk[i] = 0;
+    for (int i = lane; i < ndp; i += 32) acc[i] = make_ushort4(0, 0, 0, 0);
+    __syncwarp();
+    for (int c0 = 0; c0 < ndp; c0 += 128) {
+        int v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = c0 + 32 * u + lane;
+            v[u] = i < ndp ? order[i] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (v[u] >= 0) rk[v[u]] = uint16_t(c0 + 32 * u + lane + 1);
+    }
+    __syncwarp();
+    const int E = sh.nedges;
+    const unsigned below = (1u << lane) - 1u;
+    bool any_long = false;
+    for (int c0 = 0; c0 < E; c0 += 128) {
+        int es[4], ed[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = c0 + 32 * u + lane;
+            es[u] = e < E ? g.e_src[e] : -1;
+            ed[u] = e < E ? g.e_dst[e] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int src = es[u], dst = ed[u];
+            int rs = 0, rd = 0;
+            if (src >= 0) {
+                rs = rk[src] & 0x7FFF;
+                rd = rs > 0 ? rk[dst] & 0x7FFF : 0;
+            }
+            const bool q = rs > 0 && rd > 0;
+            const unsigned grp = __match_any_sync(kFull, q ? rd : -1 - lane);
+            int cnt = 0;
+            if (q) cnt = acc[rd - 1].w;
+            __syncwarp();
+            if (q) {
+                rk[src] = uint16_t(rs | 0x8000);  // every writer stores the same value
+                const int pos = cnt + __popc(grp & below);
+                uint16_t* a4 = reinterpret_cast<uint16_t*>(&acc[rd - 1]);
+                if (pos < 3) a4[pos] = uint16_t(rs);
+                if ((grp & below) == 0) {
+                    const int tot = cnt + __popc(grp);
+                    a4[3] = uint16_t(tot);
+                    any_long |= tot > 3;
+                }
+            }
+            __syncwarp();
+        }
+    }
+    any_long = __any_sync(kFull, any_long);
+    int list_base = 0;
+    for (int c0 = 0; c0 < ndp; c0 += 128) {
+        int v[4], code[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = c0 + 32 * u + lane;
+            v[u] = i < ndp ? order[i] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) code[u] = c0 + 32 * u + lane < ndp ? g.code[v[u]] : 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (c0 + 32 * u >= ndp) break;
+            const int i = c0 + 32 * u + lane;
+            const ushort4 dd = i < ndp ? acc[i] : make_ushort4(0, 0, 0, 0);
+            const int np = dd.w;
+            int off = 0;
+            if (any_long) {
+                int tot = 0;
+                const int cntl = (i < ndp && np > 3) ? np : 0;
+                off = list_base + warp_excl(cntl, lane, tot);
+                list_base += tot;
+                if (cntl) g.bpred[v[u]] = off;  // list cursor of the node
+            }
+            if (i < ndp) {
+                const bool sink = (rk[v[u]] & 0x8000) == 0;
+                g.sink[i] = sink ? 1 : 0;
+                // long rows: x = list offset, y = first predecessor
+                g.rowdesc[i] = make_int4(np > 3 ? off : dd.x, np > 3 ? dd.x : dd.y, dd.z,
+                                         int(uint32_t(np) | (uint32_t(sink) << 17) | (uint32_t(code[u]) << 24)));
+            }
+        }
+    }
+    __syncwarp();
+    if (any_long) {
+        for (int c0 = 0; c0 < E; c0 += 32) {
+            const int e = c0 + lane;
+            int rs = 0, dst = 0;
+            bool q = false;
+            if (e < E) {
+                dst = g.e_dst[e];
+                const int rd = rk[dst] & 0x7FFF;
+                if (rd > 0 && acc[rd - 1].w > 3) {
+                    rs = rk[g.e_src[e]] & 0x7FFF;
+                    q = rs > 0;
+                }
+            }
+            const unsigned grp = __match_any_sync(kFull, q ? dst : -1 - lane);
+            int cur = 0;
+            if (q) cur = g.bpred[dst];
+            __syncwarp();
+            if (q) {
+                g.pred_idx[cur + __popc(grp & below)] = rs;
+                if ((grp & below) == 0) g.bpred[dst] = cur + __popc(grp);
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    return true;
+}
+
 // Escape decision from H for a row of several predecessors (warp, uniform
 // arguments): the first predecessor whose diagonal gives H[i][j],
 // else the first whose vertical does, else horizontal. Returns 1000 + p,
@@ -1642,106 +1771,110 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
             order = g.dporder;
             __syncwarp();
         }
-        // Row descriptors. DP ranks of the nodes live in shared memory (the
-        // row ring is free until the DP) when they fit, else in global
-        // scratch; bit 31 marks a node with a successor among the rows.
-        int* const dpr = N <= kSmemRanks ? reinterpret_cast<int*>(ring) : g.dprank;
-        for (int i = lane; i < N; i += 32) dpr[i] = 0;
-        __syncwarp();
-        for (int i = lane; i < ndp; i += 32) dpr[order[i]] = i + 1;
-        __syncwarp();
-        // Predecessors by one pass over the edges in id order. A node's
-        // in-edge list is in edge-id order (each layer adds at most one edge
-        // into a node, with a fresh, larger id), which is spoa's predecessor
-        // order. Lanes take 32 consecutive edges; edges into the same row
-        // are ranked by lane, so the order is deterministic. rowdesc[r - 1]
-        // collects the first three predecessor ranks (x, y, z) and the count
-        // (w) of row r; bit 31 of dpr marks a node with a successor row.
-        for (int i = lane; i < ndp; i += 32) g.rowdesc[i] = make_int4(0, 0, 0, 0);
-        __syncwarp();
-        const int E = sh.nedges;
-        const unsigned below = (1u << lane) - 1u;
-        bool any_long = false;
-        for (int c0 = 0; c0 < E; c0 += 32) {
-            const int e = c0 + lane;
-            int rs = 0, rd = 0, src = 0;
-            if (e < E) {
-                src = g.e_src[e];
-                const int dst = g.e_dst[e];
-                rs = dpr[src] & 0x7FFFFFFF;
-                rd = rs > 0 ? dpr[dst] & 0x7FFFFFFF : 0;
-            }
-            const bool q = rs > 0 && rd > 0;
-            const unsigned grp = __match_any_sync(0xffffffffu, q ? rd : -1 - lane);
-            int cnt = 0;
-            if (q) {
-                atomicOr(reinterpret_cast<unsigned*>(&dpr[src]), 0x80000000u);
-                cnt = g.rowdesc[rd - 1].w;
-            }
+        // Row descriptors: shared-memory accumulators when the graph fits,
+        // else the global form below.
+        if (!descriptors_smem(g, sh, order, N, ndp, lane, ring)) {
+            // Row descriptors. DP ranks of the nodes live in shared memory (the
+            // row ring is free until the DP) when they fit, else in global
+            // scratch; bit 31 marks a node with a successor among the rows.
+            int* const dpr = N <= kSmemRanks ? reinterpret_cast<int*>(ring) : g.dprank;
+            for (int i = lane; i < N; i += 32) dpr[i] = 0;
             __syncwarp();
-            if (q) {
-                const int pos = cnt + __popc(grp & below);
-                int* rdw = reinterpret_cast<int*>(&g.rowdesc[rd - 1]);
-                if (pos < 3) rdw[pos] = rs;
-                if ((grp & below) == 0) {
-                    const int tot = cnt + __popc(grp);
-                    rdw[3] = tot;
-                    any_long |= tot > 3;
-                }
-            }
+            for (int i = lane; i < ndp; i += 32) dpr[order[i]] = i + 1;
             __syncwarp();
-        }
-        any_long = __any_sync(0xffffffffu, any_long);
-        // final descriptors; rows with more than three predecessors get their
-        // full list in pred_idx at an offset from a warp prefix of the counts
-        int list_base = 0;
-        for (int c0 = 0; c0 < ndp; c0 += 32) {
-            const int i = c0 + lane;
-            int4 dd = i < ndp ? g.rowdesc[i] : make_int4(0, 0, 0, 0);
-            const int v = i < ndp ? order[i] : 0;
-            int off = 0;
-            if (any_long) {
-                int tot = 0;
-                const int cntl = (i < ndp && dd.w > 3) ? dd.w : 0;
-                off = list_base + warp_excl(cntl, lane, tot);
-                list_base += tot;
-                if (cntl) g.bpred[v] = off;  // list cursor of the node
-            }
-            if (i < ndp) {
-                const bool sink = (dpr[v] & 0x80000000) == 0;
-                g.sink[i] = sink ? 1 : 0;
-                // long rows: x = list offset, y = first predecessor
-                g.rowdesc[i] = make_int4(dd.w > 3 ? off : dd.x, dd.w > 3 ? dd.x : dd.y, dd.z,
-                                         int(uint32_t(dd.w) | (uint32_t(sink) << 17) | (uint32_t(g.code[v]) << 24)));
-            }
-        }
-        __syncwarp();
-        if (any_long) {
-            // second pass over the edges for the long lists, same ranking
+            // Predecessors by one pass over the edges in id order. A node's
+            // in-edge list is in edge-id order (each layer adds at most one edge
+            // into a node, with a fresh, larger id), which is spoa's predecessor
+            // order. Lanes take 32 consecutive edges; edges into the same row
+            // are ranked by lane, so the order is deterministic. rowdesc[r - 1]
+            // collects the first three predecessor ranks (x, y, z) and the count
+            // (w) of row r; bit 31 of dpr marks a node with a successor row.
+            for (int i = lane; i < ndp; i += 32) g.rowdesc[i] = make_int4(0, 0, 0, 0);
+            __syncwarp();
+            const int E = sh.nedges;
+            const unsigned below = (1u << lane) - 1u;
+            bool any_long = false;
             for (int c0 = 0; c0 < E; c0 += 32) {
                 const int e = c0 + lane;
-                int rs = 0, dst = 0;
-                bool q = false;
+                int rs = 0, rd = 0, src = 0;
                 if (e < E) {
-                    dst = g.e_dst[e];
-                    const int rd = dpr[dst] & 0x7FFFFFFF;
-                    if (rd > 0 && desc_np(g.rowdesc[rd - 1].w) > 3) {
-                        rs = dpr[g.e_src[e]] & 0x7FFFFFFF;
-                        q = rs > 0;
-                    }
+                    src = g.e_src[e];
+                    const int dst = g.e_dst[e];
+                    rs = dpr[src] & 0x7FFFFFFF;
+                    rd = rs > 0 ? dpr[dst] & 0x7FFFFFFF : 0;
                 }
-                const unsigned grp = __match_any_sync(0xffffffffu, q ? dst : -1 - lane);
-                int cur = 0;
-                if (q) cur = g.bpred[dst];
+                const bool q = rs > 0 && rd > 0;
+                const unsigned grp = __match_any_sync(0xffffffffu, q ? rd : -1 - lane);
+                int cnt = 0;
+                if (q) {
+                    atomicOr(reinterpret_cast<unsigned*>(&dpr[src]), 0x80000000u);
+                    cnt = g.rowdesc[rd - 1].w;
+                }
                 __syncwarp();
                 if (q) {
-                    g.pred_idx[cur + __popc(grp & below)] = rs;
-                    if ((grp & below) == 0) g.bpred[dst] = cur + __popc(grp);
+                    const int pos = cnt + __popc(grp & below);
+                    int* rdw = reinterpret_cast<int*>(&g.rowdesc[rd - 1]);
+                    if (pos < 3) rdw[pos] = rs;
+                    if ((grp & below) == 0) {
+                        const int tot = cnt + __popc(grp);
+                        rdw[3] = tot;
+                        any_long |= tot > 3;
+                    }
                 }
                 __syncwarp();
             }
+            any_long = __any_sync(0xffffffffu, any_long);
+            // final descriptors; rows with more than three predecessors get their
+            // full list in pred_idx at an offset from a warp prefix of the counts
+            int list_base = 0;
+            for (int c0 = 0; c0 < ndp; c0 += 32) {
+                const int i = c0 + lane;
+                int4 dd = i < ndp ? g.rowdesc[i] : make_int4(0, 0, 0, 0);
+                const int v = i < ndp ? order[i] : 0;
+                int off = 0;
+                if (any_long) {
+                    int tot = 0;
+                    const int cntl = (i < ndp && dd.w > 3) ? dd.w : 0;
+                    off = list_base + warp_excl(cntl, lane, tot);
+                    list_base += tot;
+                    if (cntl) g.bpred[v] = off;  // list cursor of the node
+                }
+                if (i < ndp) {
+                    const bool sink = (dpr[v] & 0x80000000) == 0;
+                    g.sink[i] = sink ? 1 : 0;
+                    // long rows: x = list offset, y = first predecessor
+                    g.rowdesc[i] = make_int4(dd.w > 3 ? off : dd.x, dd.w > 3 ? dd.x : dd.y, dd.z,
+                                             int(uint32_t(dd.w) | (uint32_t(sink) << 17) | (uint32_t(g.code[v]) << 24)));
+                }
+            }
+            __syncwarp();
+            if (any_long) {
+                // second pass over the edges for the long lists, same ranking
+                for (int c0 = 0; c0 < E; c0 += 32) {
+                    const int e = c0 + lane;
+                    int rs = 0, dst = 0;
+                    bool q = false;
+                    if (e < E) {
+                        dst = g.e_dst[e];
+                        const int rd = dpr[dst] & 0x7FFFFFFF;
+                        if (rd > 0 && desc_np(g.rowdesc[rd - 1].w) > 3) {
+                            rs = dpr[g.e_src[e]] & 0x7FFFFFFF;
+                            q = rs > 0;
+                        }
+                    }
+                    const unsigned grp = __match_any_sync(0xffffffffu, q ? dst : -1 - lane);
+                    int cur = 0;
+                    if (q) cur = g.bpred[dst];
+                    __syncwarp();
+                    if (q) {
+                        g.pred_idx[cur + __popc(grp & below)] = rs;
+                        if ((grp & below) == 0) g.bpred[dst] = cur + __popc(grp);
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncwarp();
         }
-        __syncwarp();
         const EndCell ec = dp_dispatch(a, g, order, ndp, seq, L, lane, ring);
         cells += (unsigned long long)ndp * (unsigned long long)L;
         int iend = ec.row;
