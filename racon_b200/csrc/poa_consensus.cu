@@ -1218,18 +1218,29 @@ __device__ bool build_csr(const Graph& g, const PoaShared& sh, int lane, void* s
     c.al_x = c.in_src + E;
     c.flag = reinterpret_cast<uint8_t*>(c.al_x + A);
     // starts: exclusive prefix of the counts
+    // (graph-array loads are issued four 32-element chunks at a time)
     int bi = 0, ba = 0;
-    for (int c0 = 0; c0 < N; c0 += 32) {
-        const int v = c0 + lane;
-        int ti = 0, ta = 0;
-        const int xi = warp_excl(v < N ? g.in_cnt[v] : 0, lane, ti);
-        const int xa = warp_excl(v < N ? g.al_cnt[v] : 0, lane, ta);
-        if (v < N) {
-            c.in_off[v] = uint16_t(bi + xi);
-            c.al_off[v] = uint16_t(ba + xa);
+    for (int c4 = 0; c4 < N; c4 += 128) {
+        int ci[4], ca[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int v = c4 + 32 * u + lane;
+            ci[u] = v < N ? g.in_cnt[v] : 0;
+            ca[u] = v < N ? g.al_cnt[v] : 0;
         }
-        bi += ti;
-        ba += ta;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int v = c4 + 32 * u + lane;
+            int ti = 0, ta = 0;
+            const int xi = warp_excl(ci[u], lane, ti);
+            const int xa = warp_excl(ca[u], lane, ta);
+            if (v < N) {
+                c.in_off[v] = uint16_t(bi + xi);
+                c.al_off[v] = uint16_t(ba + xa);
+            }
+            bi += ti;
+            ba += ta;
+        }
     }
     if (lane == 0) {
         c.in_off[N] = uint16_t(E);
@@ -1239,31 +1250,47 @@ __device__ bool build_csr(const Graph& g, const PoaShared& sh, int lane, void* s
     // stable fill by owner: the offsets serve as cursors and end up at the
     // next node's start
     const unsigned below = (1u << lane) - 1u;
-    for (int c0 = 0; c0 < E; c0 += 32) {
-        const int e = c0 + lane;
-        const int dst = e < E ? g.e_dst[e] : -1 - lane;
-        const int src = e < E ? g.e_src[e] : 0;
-        const unsigned grp = __match_any_sync(0xffffffffu, dst);
-        const int cur = e < E ? c.in_off[dst] : 0;
-        __syncwarp();
-        if (e < E) {
-            c.in_src[cur + __popc(grp & below)] = uint16_t(src);
-            if ((grp & below) == 0) c.in_off[dst] = uint16_t(cur + __popc(grp));
+    for (int c4 = 0; c4 < E; c4 += 128) {
+        int ds[4], ss[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = c4 + 32 * u + lane;
+            ds[u] = e < E ? g.e_dst[e] : -1 - lane;
+            ss[u] = e < E ? g.e_src[e] : 0;
         }
-        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int dst = ds[u];
+            const unsigned grp = __match_any_sync(0xffffffffu, dst);
+            const int cur = dst >= 0 ? c.in_off[dst] : 0;
+            __syncwarp();
+            if (dst >= 0) {
+                c.in_src[cur + __popc(grp & below)] = uint16_t(ss[u]);
+                if ((grp & below) == 0) c.in_off[dst] = uint16_t(cur + __popc(grp));
+            }
+            __syncwarp();
+        }
     }
-    for (int c0 = 0; c0 < A; c0 += 32) {
-        const int x = c0 + lane;
-        const int own = x < A ? g.a_owner[x] : -1 - lane;
-        const int y = x < A ? g.a_node[x] : 0;
-        const unsigned grp = __match_any_sync(0xffffffffu, own);
-        const int cur = x < A ? c.al_off[own] : 0;
-        __syncwarp();
-        if (x < A) {
-            c.al_x[cur + __popc(grp & below)] = uint16_t(y);
-            if ((grp & below) == 0) c.al_off[own] = uint16_t(cur + __popc(grp));
+    for (int c4 = 0; c4 < A; c4 += 128) {
+        int os[4], ys[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int x = c4 + 32 * u + lane;
+            os[u] = x < A ? g.a_owner[x] : -1 - lane;
+            ys[u] = x < A ? g.a_node[x] : 0;
         }
-        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int own = os[u];
+            const unsigned grp = __match_any_sync(0xffffffffu, own);
+            const int cur = own >= 0 ? c.al_off[own] : 0;
+            __syncwarp();
+            if (own >= 0) {
+                c.al_x[cur + __popc(grp & below)] = uint16_t(ys[u]);
+                if ((grp & below) == 0) c.al_off[own] = uint16_t(cur + __popc(grp));
+            }
+            __syncwarp();
+        }
     }
     // shift the cursors back to starts (off[v] = end of v - 1), top chunk first
     for (int c0 = ((N - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
@@ -1537,6 +1564,146 @@ __device__ bool descriptors_smem(const Graph& g, const PoaShared& sh, const int*
     }
     __syncwarp();
     return true;
+}
+
+// Heaviest bundle (g_heaviest_bundle) with the scores in shared memory: per
+// node an int32 score and a uint16 predecessor, and for each chunk of 32 ranks
+// the in-edges (source, weight) staged by the lanes in parallel, so the
+// serial pass of lane 0 touches no global memory. Scores are bounded by
+// sequences x 186 x nodes (two Phred values per sequence and edge, summed
+// along a path), checked against int32. When branch completion is needed, or
+// the graph does not fit, the global form finishes or does the work.
+// Warp-collective; returns the path length (-1 on failure) on every lane.
+__device__ int heaviest_bundle_warp(const Graph& g, PoaShared& sh, int lane, int4* ring) {
+    constexpr int D = 8;  // staged in-edges per node
+    const int N = sh.nnodes, R = sh.nranks;
+    uint8_t* base = reinterpret_cast<uint8_t*>(ring);
+    int* const bs = reinterpret_cast<int*>(base);                             // [N]
+    uint16_t* const bp = reinterpret_cast<uint16_t*>(base + 4 * size_t(N));   // [N], 0xFFFF = none
+    const size_t st_off = (6 * size_t(N) + 15) & ~size_t(15);
+    int* const sw = reinterpret_cast<int*>(base + st_off);                    // [32][D] weights
+    uint16_t* const su = reinterpret_cast<uint16_t*>(sw + 32 * D);            // [32][D] sources
+    int* const sv = reinterpret_cast<int*>(su + 32 * D);                      // [32] node
+    int* const sd = sv + 32;                                                  // [32] degree, D + 1 = more
+    const size_t need = st_off + 32 * D * 6 + 32 * 8;
+    const bool fits = N < 65535 && need <= size_t(kRingBytesPerWarp) &&
+                      double(sh.nseq + 1) * 186.0 * double(N + 1) < 2.0e9;
+    if (!fits) {
+        int len = 0;
+        if (lane == 0) len = g_heaviest_bundle(g, sh);
+        return __shfl_sync(0xffffffffu, len, 0);
+    }
+    for (int i = lane; i < N; i += 32) {
+        bs[i] = -1;
+        bp[i] = 0xFFFF;
+    }
+    __syncwarp();
+    int best_id = 0;
+    for (int r0 = 0; r0 < R; r0 += 32) {
+        const int r = r0 + lane;
+        if (r < R) {
+            const int v = g.rank_to_node[r];
+            int deg = 0;
+            for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e]) {
+                if (deg == D) {
+                    deg = D + 1;
+                    break;
+                }
+                su[lane * D + deg] = uint16_t(g.e_src[e]);
+                sw[lane * D + deg] = g.e_w[e];
+                ++deg;
+            }
+            sv[lane] = v;
+            sd[lane] = deg;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int cnt = min(32, R - r0);
+            for (int t = 0; t < cnt; ++t) {
+                const int v = sv[t];
+                const int deg = sd[t];
+                int sv_ = bs[v], pv_ = bp[v] == 0xFFFF ? -1 : int(bp[v]);
+                auto consider = [&](int u, int w) {
+                    if (sv_ < w || (sv_ == w && pv_ != -1 && bs[pv_] <= bs[u])) {
+                        sv_ = w;
+                        pv_ = u;
+                    }
+                };
+                if (deg <= D) {
+                    for (int q = 0; q < deg; ++q) consider(su[t * D + q], sw[t * D + q]);
+                } else {
+                    for (int e = g.in_head[v]; e != -1; e = g.e_next_in[e]) consider(g.e_src[e], g.e_w[e]);
+                }
+                if (pv_ != -1) sv_ += bs[pv_];
+                bs[v] = sv_;
+                bp[v] = pv_ < 0 ? uint16_t(0xFFFF) : uint16_t(pv_);
+                if (bs[best_id] < sv_) best_id = v;
+            }
+        }
+        __syncwarp();
+    }
+    best_id = __shfl_sync(0xffffffffu, best_id, 0);
+    const bool complete = g.out_head[best_id] != -1;
+    if (complete) {
+        // branch completion works on the global arrays
+        for (int i = lane; i < N; i += 32) {
+            g.bscore[i] = bs[i];
+            g.bpred[i] = bp[i] == 0xFFFF ? -1 : int(bp[i]);
+        }
+        __syncwarp();
+        int len = 0;
+        if (lane == 0) {
+            for (int r = 0; r < R; ++r) g.node_rank[g.rank_to_node[r]] = r;
+            int guard = 0;
+            len = 1;
+            while (g.out_head[best_id] != -1) {
+                best_id = g_branch_completion(g, sh, g.node_rank[best_id]);
+                if (++guard > N + 1) {
+                    len = -1;
+                    break;
+                }
+            }
+            if (len > 0) {
+                len = 0;
+                while (g.bpred[best_id] != -1) {
+                    g.cons[len++] = best_id;
+                    best_id = g.bpred[best_id];
+                    if (len > N) {
+                        len = -1;
+                        break;
+                    }
+                }
+                if (len >= 0) g.cons[len++] = best_id;
+            }
+            for (int i = 0, j = len - 1; i < j; ++i, --j) {
+                const int t = g.cons[i];
+                g.cons[i] = g.cons[j];
+                g.cons[j] = t;
+            }
+        }
+        return __shfl_sync(0xffffffffu, len, 0);
+    }
+    int len = 0;
+    if (lane == 0) {
+        int v = best_id;
+        while (bp[v] != 0xFFFF) {
+            g.cons[len++] = v;
+            v = bp[v];
+            if (len > N) {
+                len = -1;
+                break;
+            }
+        }
+        if (len >= 0) {
+            g.cons[len++] = v;
+            for (int i = 0, j = len - 1; i < j; ++i, --j) {
+                const int t = g.cons[i];
+                g.cons[i] = g.cons[j];
+                g.cons[j] = t;
+            }
+        }
+    }
+    return __shfl_sync(0xffffffffu, len, 0);
 }
 
 // Escape decision from H for a row of several predecessors (warp, uniform
@@ -1945,8 +2112,9 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         g.bpred[i] = -1;
     }
     __syncwarp();
+    const int hb_len = heaviest_bundle_warp(g, sh, lane, ring);
     if (lane == 0) {
-        const int len = g_heaviest_bundle(g, sh);
+        const int len = hb_len;
         uint8_t flags = kPolished;
         if (len < 0) {
             flags = kFailed;
