@@ -2362,7 +2362,11 @@ void PoaEngine::run(bool plain) {
     const uint32_t* h_order = h_order_.as<uint32_t>();
     // batched form: size-sorted queue; plain form: input order
     for (size_t i = 0; i < n; ++i) todo[i] = plain ? uint32_t(i) : h_order[i];
+    // starting graph capacity; windows that outgrow it run again with four
+    // times as much. RB_POA_NCAP lowers the start (tests of the retry path);
+    // results do not depend on it.
     int ncap = 4096;
+    if (const char* e = getenv("RB_POA_NCAP")) ncap = std::max(256, std::min(4096, atoi(e)));
     std::vector<uint8_t> flags(n);
     float total_ms = 0;
     // DP row width: every layer's columns rounded up to whole warp passes
