@@ -40,6 +40,10 @@ namespace {
 // minus infinity that survives thousands of gap additions without overflow
 constexpr int kNegInf = -(1 << 29);
 constexpr uint64_t kNoQual = ~0ull;
+// per-warp shared memory: the DP row ring, reused by the other steps
+constexpr int kRingBytesPerWarp = 16384;
+// node ranks held in the ring's shared memory during the descriptor build
+constexpr int kSmemRanks = (kRingBytesPerWarp - 512) / 4;
 
 enum PoaFlag : uint8_t {
     kPolished = 1,
@@ -108,7 +112,7 @@ struct Graph {
     uint8_t* dec;
     // per-node in-edge and aligned-entry counts, owner node of each aligned
     // entry (for the compact lists built in shared memory)
-    int *in_cnt, *al_cnt, *a_owner;
+    int *in_cnt, *al_cnt, *a_owner, *out_cnt;
     int ncap, ecap, acap, scap, lcap, alncap;
 };
 
@@ -179,6 +183,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(N * 4, 40);       // in_cnt
     take(N * 4, 41);       // al_cnt
     take(A * 4, 42);       // a_owner
+    take(N * 4, 43);       // out_cnt
     take((N + 2) * 4, 24); // pred_off
     take((E + N + 2) * 4, 25);  // pred_idx
     take((N + L + 2) * 4, 26);  // aln_node
@@ -197,7 +202,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
 __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
     uint8_t* base = a.scratch + size_t(slot) * a.slot_bytes;
     Graph g;
-    void* p[43];
+    void* p[44];
     walk_layout(a.ncap, a.ecap, a.acap, a.lcap, [&](int id, size_t off) { p[id] = base + off; });
     g.code = (uint8_t*)p[0];
     g.cov = (uint32_t*)p[1];
@@ -242,6 +247,7 @@ __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
     g.in_cnt = (int*)p[40];
     g.al_cnt = (int*)p[41];
     g.a_owner = (int*)p[42];
+    g.out_cnt = (int*)p[43];
     g.ncap = a.ncap;
     g.ecap = a.ecap;
     g.acap = a.acap;
@@ -384,6 +390,74 @@ __device__ __forceinline__ int warp_excl(int v, int lane, int& total) {
     return x - v;
 }
 
+// Out-edges of nodes [0, N) as uint16 lists in shared memory: destination and
+// edge id, grouped by source (order within a source is irrelevant: the lists
+// answer "does u -> v exist, and which edge is it"). Loads of the edge
+// arrays go four 32-edge chunks at a time. Returns false, building nothing,
+// when the lists do not fit in `cap` bytes or 16-bit indices.
+struct OutCsr {
+    uint16_t* off;  // [N + 1]
+    uint16_t* dst;  // [E]
+    uint16_t* eid;  // [E]
+};
+__device__ bool build_out_csr(const Graph& g, int N, int E, int lane, void* smem, int cap, OutCsr& c) {
+    if (N >= 65535 || E >= 65535 || 2 * (size_t(N) + 1) + 4 * size_t(E) > size_t(cap)) return false;
+    c.off = reinterpret_cast<uint16_t*>(smem);
+    c.dst = c.off + (N + 1);
+    c.eid = c.dst + E;
+    int b = 0;
+    for (int c4 = 0; c4 < N; c4 += 128) {
+        int cn[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int v = c4 + 32 * u + lane;
+            cn[u] = v < N ? g.out_cnt[v] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int v = c4 + 32 * u + lane;
+            int t = 0;
+            const int x = warp_excl(cn[u], lane, t);
+            if (v < N) c.off[v] = uint16_t(b + x);
+            b += t;
+        }
+    }
+    if (lane == 0) c.off[N] = uint16_t(E);
+    __syncwarp();
+    const unsigned below = (1u << lane) - 1u;
+    for (int c4 = 0; c4 < E; c4 += 128) {
+        int ss[4], ds[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int e = c4 + 32 * u + lane;
+            ss[u] = e < E ? g.e_src[e] : -1 - lane;
+            ds[u] = e < E ? g.e_dst[e] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int src = ss[u];
+            const unsigned grp = __match_any_sync(0xffffffffu, src);
+            const int cur = src >= 0 ? c.off[src] : 0;
+            __syncwarp();
+            if (src >= 0) {
+                const int q = cur + __popc(grp & below);
+                c.dst[q] = uint16_t(ds[u]);
+                c.eid[q] = uint16_t(c4 + 32 * u + lane);
+                if ((grp & below) == 0) c.off[src] = uint16_t(cur + __popc(grp));
+            }
+            __syncwarp();
+        }
+    }
+    for (int c0 = ((N - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
+        const int v = c0 + lane;
+        const uint16_t pv = (v < N && v > 0) ? c.off[v - 1] : uint16_t(0);
+        __syncwarp();
+        if (v < N) c.off[v] = pv;
+        __syncwarp();
+    }
+    return true;
+}
+
 // Graph::add_alignment for one layer, by the whole warp. A path visits every
 // node and every aligned group at most once, so the per-position work is
 // independent: classify each aligned base (existing node, new base, new
@@ -395,7 +469,7 @@ __device__ __forceinline__ int warp_excl(int v, int lane, int& total) {
 // order_insert). Per-entry scratch lives in g.stack: [0,m) node, [m,2m) kind
 // | aligned-count << 2, [2m,3m) anchor slot, [3m,4m) group start.
 __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t* seq, const uint8_t* qual,
-                                   int len, int lane) {
+                                   int len, int lane, int4* ring) {
     const int m = sh.naln;
     const int nold = sh.nnodes;
     if (len == 0) return;
@@ -410,30 +484,61 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
     int* e_start = g.stack + 3 * m;
     const int first_pos = g.aln_pos[m - 1], last_pos = g.aln_pos[0];
     const int h = first_pos, tl = len - 1 - last_pos;
-    // 1. classify (reads only the graph as it was before this insertion)
-    for (int t = lane; t < m; t += 32) {
-        const int k = m - 1 - t;
-        const int at = g.aln_node[k];
-        const uint8_t letter = seq[g.aln_pos[k]];
-        int kind = 1, nid = -1, nal = 0, slot = INT_MIN, start = INT_MAX;
-        if (at != -1) {
-            slot = group_end_rank(g, at, nold);
-            start = group_start_rank(g, at, nold);
-            if (g.code[at] == letter) {
-                kind = 0;
-                nid = at;
-            } else {
-                for (int x = g.al_head[at]; x != -1; x = g.a_next[x]) {
-                    ++nal;
-                    if (nid == -1 && g.code[g.a_node[x]] == letter) nid = g.a_node[x];
-                }
-                kind = nid == -1 ? 2 : 0;
-            }
+    // existing-edge lookups of step 5 from shared memory when they fit
+    OutCsr oc;
+    const bool ocsr = build_out_csr(g, nold, sh.nedges, lane, ring, kRingBytesPerWarp, oc);
+    // 1. classify (reads only the graph as it was before this insertion);
+    //    the loads of four 32-entry chunks go out together
+    for (int t4 = 0; t4 < m; t4 += 128) {
+        int at[4], pos[4], cd[4], rk[4], ah[4];
+        uint8_t letter[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = t4 + 32 * u + lane;
+            at[u] = t < m ? g.aln_node[m - 1 - t] : -1;
+            pos[u] = t < m ? g.aln_pos[m - 1 - t] : 0;
         }
-        e_nid[t] = nid;
-        e_kind[t] = kind | (kind == 2 ? nal << 2 : 0);
-        e_slot[t] = slot;
-        e_start[t] = start;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = t4 + 32 * u + lane;
+            letter[u] = t < m ? seq[pos[u]] : 0;
+            cd[u] = at[u] >= 0 ? g.code[at[u]] : -1;
+            rk[u] = at[u] >= 0 ? g.my_rank[at[u]] : 0;
+            ah[u] = at[u] >= 0 ? g.al_head[at[u]] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = t4 + 32 * u + lane;
+            if (t >= m) continue;
+            int kind = 1, nid = -1, nal = 0, slot = INT_MIN, start = INT_MAX;
+            if (at[u] != -1) {
+                // the group's rank extent (group_end_rank / group_start_rank)
+                slot = start = rk[u];
+                const bool same = cd[u] == int(letter[u]);
+                for (int x = ah[u]; x != -1; x = g.a_next[x]) {
+                    const int y = g.a_node[x];
+                    if (y < nold) {
+                        const int ry = g.my_rank[y];
+                        slot = max(slot, ry);
+                        start = min(start, ry);
+                    }
+                    if (!same) {
+                        ++nal;
+                        if (nid == -1 && g.code[y] == letter[u]) nid = y;
+                    }
+                }
+                if (same) {
+                    kind = 0;
+                    nid = at[u];
+                } else {
+                    kind = nid == -1 ? 2 : 0;
+                }
+            }
+            e_nid[t] = nid;
+            e_kind[t] = kind | (kind == 2 ? nal << 2 : 0);
+            e_slot[t] = slot;
+            e_start[t] = start;
+        }
     }
     __syncwarp();
     // 2. ids of new aligned bases, aligned-pool offsets, order slots
@@ -502,6 +607,7 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
         g.al_head[id] = g.al_tail[id] = -1;
         g.in_cnt[id] = 0;
         g.al_cnt[id] = 0;
+        g.out_cnt[id] = 0;
     }
     __syncwarp();
     for (int t = lane; t < m; t += 32) {
@@ -543,12 +649,21 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
             u = path_node(k - 1);
             v = path_node(k);
             w = layer_weight(qual, k - 1) + layer_weight(qual, k);
-            if (u < nold)
-                for (int e = g.out_head[u]; e != -1; e = g.e_next_out[e])
-                    if (g.e_dst[e] == v) {
-                        found = e;
-                        break;
-                    }
+            if (u < nold && v < nold) {
+                if (ocsr) {
+                    for (int q = oc.off[u], qe = oc.off[u + 1]; q < qe; ++q)
+                        if (oc.dst[q] == v) {
+                            found = oc.eid[q];
+                            break;
+                        }
+                } else {
+                    for (int e = g.out_head[u]; e != -1; e = g.e_next_out[e])
+                        if (g.e_dst[e] == v) {
+                            found = e;
+                            break;
+                        }
+                }
+            }
         }
         int tot;
         const int pre = warp_excl((k < len && found < 0) ? 1 : 0, lane, tot);
@@ -570,6 +685,7 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
                 else g.e_next_in[g.in_tail[v]] = id;
                 g.in_tail[v] = id;
                 g.in_cnt[v] += 1;  // at most one new edge into v per layer
+                g.out_cnt[u] += 1;  // and at most one out of u
             }
         }
         new_edges += tot;
@@ -895,9 +1011,6 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
                    __shfl_sync(kFull, ties, lane_l)};
 }
 
-constexpr int kRingBytesPerWarp = 16384;
-// node ranks held in the ring's shared memory during the descriptor build
-constexpr int kSmemRanks = (kRingBytesPerWarp - 512) / 4;
 // last 512 bytes of each warp's ring hold the 32-row descriptor block
 constexpr int kRingDescOffset = (kRingBytesPerWarp - 512) / 16;
 
@@ -1891,6 +2004,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         g.my_rank[i] = i;
         g.in_cnt[i] = i > 0 ? 1 : 0;
         g.al_cnt[i] = 0;
+        g.out_cnt[i] = i + 1 < B ? 1 : 0;
     }
     if (lane == 0) {
         sh.nnodes = B;
@@ -2084,7 +2198,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         }
         __syncwarp();
         if (sh.fail) break;
-        add_alignment_warp(g, sh, seq, qual, L, lane);
+        add_alignment_warp(g, sh, seq, qual, L, lane, ring);
         if (sh.fail) break;
         order_insert(g, sh, N, lane);
     }
