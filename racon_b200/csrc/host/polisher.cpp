@@ -114,50 +114,121 @@ size_t name_end(const std::string& s, size_t from) {
     return e;
 }
 
-void append_residues(std::string& dst, const std::string& line) {
-    for (char c : line)
-        if (!isspace(uint8_t(c))) dst.push_back(c);
+// Whole file (gzip or plain) in memory; plain files by one fread.
+std::string slurp(const std::string& path, bool& ok) {
+    std::string buf;
+    if (FILE* pf = fopen(path.c_str(), "rb")) {
+        unsigned char magic[2] = {0, 0};
+        const size_t got = fread(magic, 1, 2, pf);
+        if (!(got == 2 && magic[0] == 0x1f && magic[1] == 0x8b) && fseek(pf, 0, SEEK_END) == 0) {
+            const long size = ftell(pf);
+            if (size >= 0 && fseek(pf, 0, SEEK_SET) == 0) {
+                buf.resize(size_t(size));
+                const size_t r = size ? fread(&buf[0], 1, size_t(size), pf) : 0;
+                fclose(pf);
+                ok = r == size_t(size);
+                return buf;
+            }
+        }
+        fclose(pf);
+    }
+    gzFile f = gzopen(path.c_str(), "rb");
+    ok = f != nullptr;
+    if (!f) return buf;
+    gzbuffer(f, 1 << 20);
+    const size_t chunk = size_t(16) << 20;
+    size_t len = 0;
+    while (true) {
+        buf.resize(len + chunk);
+        const int r = gzread(f, &buf[len], unsigned(chunk));
+        if (r <= 0) break;
+        len += size_t(r);
+    }
+    buf.resize(len);
+    gzclose(f);
+    return buf;
+}
+
+inline bool is_space(char c) { return c == ' ' || (c >= '\t' && c <= '\r'); }
+
+// Appends [b, e) without whitespace; a whole-line append when there is none
+// (the check is a branch-free loop the compiler vectorises).
+void append_clean(std::string& dst, const char* b, const char* e) {
+    bool any = false;
+    for (const char* p = b; p < e; ++p) any |= is_space(*p);
+    if (!any) {
+        dst.append(b, size_t(e - b));
+        return;
+    }
+    for (const char* p = b; p < e; ++p)
+        if (!is_space(*p)) dst.push_back(*p);
+}
+
+// Line cursor over an in-memory file: [b, e) of the next line without '\n'
+// and a trailing '\r'.
+struct LineCursor {
+    const char* p;
+    const char* end;
+    bool next(const char*& b, const char*& e) {
+        if (p >= end) return false;
+        b = p;
+        const char* nl = static_cast<const char*>(memchr(p, '\n', size_t(end - p)));
+        e = nl ? nl : end;
+        p = nl ? nl + 1 : end;
+        if (e > b && e[-1] == '\r') --e;
+        return true;
+    }
+};
+
+size_t name_len(const char* b, const char* e) {
+    const char* q = b;
+    while (q < e && !isspace(uint8_t(*q))) ++q;
+    return size_t(q - b);
 }
 
 void read_sequences(const std::string& path, int format, std::vector<std::unique_ptr<Sequence>>& dst) {
-    Lines in(path);
-    if (!in.ok()) fail("[racon::Polisher::initialize] error: unable to open file " + path + "!");
-    std::string line, name, data, qual;
+    bool ok = false;
+    const std::string buf = slurp(path, ok);
+    if (!ok) fail("[racon::Polisher::initialize] error: unable to open file " + path + "!");
+    LineCursor in{buf.data(), buf.data() + buf.size()};
+    const char *b, *e;
+    std::string data, qual;
     if (format == 0) {
         bool open = false;
-        while (in.next(line)) {
-            if (!line.empty() && line[0] == '>') {
-                if (open)
-                    dst.emplace_back(new Sequence(name.data(), uint32_t(name.size()), data.data(),
-                                                  uint32_t(data.size())));
-                name.assign(line, 1, name_end(line, 1) - 1);
+        const char* nb = nullptr;
+        size_t nl = 0;
+        while (in.next(b, e)) {
+            if (e > b && *b == '>') {
+                if (open) dst.emplace_back(new Sequence(nb, uint32_t(nl), data.data(), uint32_t(data.size())));
+                nb = b + 1;
+                nl = name_len(b + 1, e);
                 data.clear();
                 open = true;
             } else if (open) {
-                append_residues(data, line);
+                append_clean(data, b, e);
             }
         }
-        if (open)
-            dst.emplace_back(new Sequence(name.data(), uint32_t(name.size()), data.data(), uint32_t(data.size())));
+        if (open) dst.emplace_back(new Sequence(nb, uint32_t(nl), data.data(), uint32_t(data.size())));
         return;
     }
-    while (in.next(line)) {
-        if (line.empty() || line[0] != '@') continue;
-        name.assign(line, 1, name_end(line, 1) - 1);
+    while (in.next(b, e)) {
+        if (e == b || *b != '@') continue;
+        const char* nb = b + 1;
+        const size_t nl = name_len(b + 1, e);
         data.clear();
         qual.clear();
         bool plus = false;
-        while (in.next(line)) {
-            if (!line.empty() && line[0] == '+') {
+        while (in.next(b, e)) {
+            if (e > b && *b == '+') {
                 plus = true;
                 break;
             }
-            append_residues(data, line);
+            append_clean(data, b, e);
         }
         if (!plus) fail("[racon::Polisher::initialize] error: truncated FASTQ record in " + path + "!");
-        while (qual.size() < data.size() && in.next(line)) append_residues(qual, line);
-        dst.emplace_back(new Sequence(name.data(), uint32_t(name.size()), data.data(), uint32_t(data.size()),
-                                      qual.data(), uint32_t(qual.size())));
+        while (qual.size() < data.size() && in.next(b, e)) append_clean(qual, b, e);
+        dst.emplace_back(new Sequence(nb, uint32_t(nl), data.data(), uint32_t(data.size()), qual.data(),
+                                      uint32_t(qual.size())));
     }
 }
 
@@ -170,7 +241,12 @@ uint32_t to_u32(const std::string& s) { return uint32_t(strtoul(s.c_str(), nullp
 Sequence::Sequence(const char* name, uint32_t name_length, const char* data, uint32_t data_length)
     : name_(name, name_length) {
     data_.resize(data_length);
-    for (uint32_t i = 0; i < data_length; ++i) data_[i] = char(toupper(uint8_t(data[i])));
+    // toupper in the C locale: only a-z change
+    char* d = &data_[0];
+    for (uint32_t i = 0; i < data_length; ++i) {
+        const char c = data[i];
+        d[i] = (c >= 'a' && c <= 'z') ? char(c - 32) : c;
+    }
 }
 
 Sequence::Sequence(const char* name, uint32_t name_length, const char* data, uint32_t data_length,
@@ -189,18 +265,20 @@ std::unique_ptr<Sequence> createSequence(const std::string& name, const std::str
 
 void Sequence::create_reverse_complement() {
     if (!reverse_complement_.empty()) return;
-    reverse_complement_.resize(data_.size());
-    for (size_t i = 0, n = data_.size(); i < n; ++i) {
-        char c = data_[n - 1 - i];
-        switch (c) {
-            case 'A': c = 'T'; break;
-            case 'T': c = 'A'; break;
-            case 'C': c = 'G'; break;
-            case 'G': c = 'C'; break;
-            default: break;
+    // A <-> T, C <-> G, every other byte unchanged (src/sequence.cpp:49-84)
+    static const struct Table {
+        char t[256];
+        Table() {
+            for (int c = 0; c < 256; ++c) t[c] = char(c);
+            t[uint8_t('A')] = 'T';
+            t[uint8_t('T')] = 'A';
+            t[uint8_t('C')] = 'G';
+            t[uint8_t('G')] = 'C';
         }
-        reverse_complement_[i] = c;
-    }
+    } comp;
+    reverse_complement_.resize(data_.size());
+    char* r = &reverse_complement_[0];
+    for (size_t i = 0, n = data_.size(); i < n; ++i) r[i] = comp.t[uint8_t(data_[n - 1 - i])];
     reverse_quality_.assign(quality_.rbegin(), quality_.rend());
 }
 
