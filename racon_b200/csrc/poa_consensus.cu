@@ -727,33 +727,55 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
 // Splices the new nodes of the last insertion into the incremental order
 // (warp): an old node at rank r moves up by the number of new nodes with slot
 // < r, the k-th new node (slots sorted) lands at slot + 1 + k.
-__device__ void order_insert(const Graph& g, const PoaShared& sh, int nold, int lane) {
+__device__ void order_insert(const Graph& g, const PoaShared& sh, int nold, int lane, int4* ring) {
     const int nnew = sh.nnew, n = nold + nnew;
-    for (int r = lane; r <= nold; r += 32) g.shift[r] = 0;
+    // shift counts in shared memory when they fit (the ring is free here)
+    int* const shift = size_t(nold + 1) * 4 <= size_t(kRingBytesPerWarp) ? reinterpret_cast<int*>(ring) : g.shift;
+    for (int r = lane; r <= nold; r += 32) shift[r] = 0;
     __syncwarp();
     for (int k = lane; k < nnew; k += 32) {
         const int at = g.nw_slot[k] + 1;
-        if (at < nold) atomicAdd(&g.shift[at], 1);
+        if (at < nold) atomicAdd(&shift[at], 1);
     }
     __syncwarp();
     int base = 0;
-    for (int c0 = 0; c0 < nold; c0 += 32) {
-        const int r = c0 + lane;
-        int v = r < nold ? g.shift[r] : 0;
+    for (int c4 = 0; c4 < nold; c4 += 128) {
+        int ov[4];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane >= o) v += y;
+        for (int u = 0; u < 4; ++u) {
+            const int r = c4 + 32 * u + lane;
+            ov[u] = r < nold ? g.ord[r] : 0;
         }
-        if (r < nold) g.ord2[r + base + v] = g.ord[r];
-        base += __shfl_sync(0xffffffffu, v, 31);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int r = c4 + 32 * u + lane;
+            int v = r < nold ? shift[r] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += y;
+            }
+            if (r < nold) g.ord2[r + base + v] = ov[u];
+            base += __shfl_sync(0xffffffffu, v, 31);
+        }
     }
     for (int k = lane; k < nnew; k += 32) g.ord2[g.nw_slot[k] + 1 + k] = g.nw_node[k];
     __syncwarp();
-    for (int x = lane; x < n; x += 32) {
-        const int v = g.ord2[x];
-        g.ord[x] = v;
-        g.my_rank[v] = x;
+    for (int x4 = 0; x4 < n; x4 += 128) {
+        int vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int x = x4 + 32 * u + lane;
+            vv[u] = x < n ? g.ord2[x] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int x = x4 + 32 * u + lane;
+            if (x < n) {
+                g.ord[x] = vv[u];
+                g.my_rank[vv[u]] = x;
+            }
+        }
     }
     __syncwarp();
 }
@@ -2039,14 +2061,25 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         int ndp = N;
         const int* order = g.ord;
         if (!full) {
+            // compaction of the member nodes in order; the loads of four
+            // 32-entry chunks go out together
             int base = 0;
-            for (int c0 = 0; c0 < N; c0 += 32) {
-                const int r = c0 + lane;
-                const int v = r < N ? g.ord[r] : 0;
-                const bool in = r < N && g.member[v];
-                const unsigned m = __ballot_sync(0xffffffffu, in);
-                if (in) g.dporder[base + __popc(m & ((1u << lane) - 1u))] = v;
-                base += __popc(m);
+            for (int c4 = 0; c4 < N; c4 += 128) {
+                int vv[4];
+                bool in[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int r = c4 + 32 * u + lane;
+                    vv[u] = r < N ? g.ord[r] : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) in[u] = c4 + 32 * u + lane < N && g.member[vv[u]];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const unsigned m = __ballot_sync(0xffffffffu, in[u]);
+                    if (in[u]) g.dporder[base + __popc(m & ((1u << lane) - 1u))] = vv[u];
+                    base += __popc(m);
+                }
             }
             ndp = base;
             order = g.dporder;
@@ -2200,7 +2233,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         if (sh.fail) break;
         add_alignment_warp(g, sh, seq, qual, L, lane, ring);
         if (sh.fail) break;
-        order_insert(g, sh, N, lane);
+        order_insert(g, sh, N, lane, ring);
     }
     // spoa's topological order of the final graph for the consensus
     if (!sh.fail) {
