@@ -2194,9 +2194,36 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         int iend = ec.row;
         if (ec.ties > 1) {
             // several sinks share the best last-column value: spoa takes the
-            // first in its own topological order of the aligned (sub)graph
-            const int nr = topo_sort_warp(g, sh, full, g.rank_to_node, lane, ring);
-            if (nr < 0) {
+            // first in its own topological order of the aligned (sub)graph.
+            // A sink outside every aligned group is reached by spoa's DFS
+            // only as a root (no member lists it as an in-edge tail, and
+            // aligned links are symmetric), so such sinks are ranked by node
+            // id; only a tie that involves an aligned sink needs the DFS.
+            int low_id = INT_MAX, low_i = iend;
+            bool grouped = false;
+            for (int i = 1 + lane; i <= ndp; i += 32) {
+                if (!g.sink[i - 1] || g.H[i * g.lcap + L] != ec.value) continue;
+                const int v = order[i - 1];
+                grouped |= g.al_cnt[v] != 0;
+                if (v < low_id) {
+                    low_id = v;
+                    low_i = i;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const int ov = __shfl_xor_sync(0xffffffffu, low_id, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, low_i, o);
+                if (ov < low_id) {
+                    low_id = ov;
+                    low_i = oi;
+                }
+            }
+            grouped = __any_sync(0xffffffffu, grouped);
+            const int nr = grouped ? topo_sort_warp(g, sh, full, g.rank_to_node, lane, ring) : 0;
+            if (!grouped) {
+                iend = low_i;
+            } else if (nr < 0) {
                 if (lane == 0) sh.fail = kOverflow;
             } else {
                 for (int r = lane; r < nr; r += 32) g.node_rank[g.rank_to_node[r]] = r;
