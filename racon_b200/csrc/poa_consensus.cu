@@ -3,24 +3,29 @@
 // over spoa's partial-order graph (linear-gap NW, match/mismatch/gap from
 // racon's -m/-x/-g, engine built at src/polisher.cpp:181-185).
 //
-// Design (B200, sm_100a). One CTA owns one window at a time; CTAs are
-// persistent and pull windows from a size-sorted queue. Each CTA has a slot of
-// global scratch holding the window's graph (node/edge arrays with ordered
-// in/out/aligned lists), the DP matrix and the traceback decisions.
-// * Graph maintenance (insertion of an aligned layer, the DFS topological order
-//   with aligned groups kept adjacent, subgraph extraction, heaviest-bundle
-//   consensus) is inherently sequential pointer work and runs on thread 0.
-// * The DP of one layer against the (sub)graph runs on all threads, one row
-//   (graph node in topological order) at a time: the diagonal and vertical
-//   terms over the predecessors are independent per column, the in-row gap
-//   term H[i][j] = max(T[j], H[i][j-1] + g) is a max-plus prefix scan done as
-//   a per-thread segment scan followed by a block-wide scan of segment
-//   carries. The traceback decision of every cell (first predecessor giving
-//   the diagonal value, else first giving the vertical value, else
-//   horizontal) is computed in the same pass, so the walk back reads one byte
-//   per step.
-// * The NW end cell is the first sink, in topological order, with the best
-//   last-column score (block reduction with rank tie-break).
+// Design (B200, sm_100a). One warp owns one window at a time; warps (4 per
+// CTA, 12 per SM) are persistent and pull windows from a size-sorted queue.
+// Each warp has a slot of global scratch (graph arrays first, then the DP
+// score rows and decision bit-planes) and a 16 KB shared-memory ring.
+// * Per layer: the subgraph of a partial layer, row descriptors (first
+//   predecessor ranks, count, sink flag, base), the DP, the end cell, the
+//   traceback and the insertion of the aligned layer, all warp-cooperative.
+//   The steps that walk the graph build compact uint16 adjacency lists or
+//   accumulators in the shared ring when they fit, so their dependent steps
+//   read shared memory; loads of graph arrays go out 128 entries at a time.
+// * The DP runs one row (graph node in a valid topological order kept
+//   incrementally) at a time: lane l owns S consecutive columns, recent rows
+//   sit in the ring, diagonal and vertical terms take the max over the
+//   predecessors (DPX add-max forms), and the in-row gap term H[i][j] =
+//   max(T[j], H[i][j-1] + g) is a max-plus prefix (in-lane sub-chains, warp
+//   scan). Decisions are two bit-planes per lane and row; the walk decides
+//   the rare remaining cells again from the stored scores, in spoa's order
+//   (diagonal through each predecessor, then vertical, then horizontal).
+// * The NW end cell is the first sink in spoa's topological order with the
+//   best last-column score; spoa's DFS order is built only when tied sinks
+//   belong to aligned groups.
+// * After the last layer: spoa's topological order, heaviest bundle (scores
+//   in shared memory), branch completion, coverages and trimming.
 // Exact int32 arithmetic throughout; results are byte-identical to the CPU
 // algorithm by construction.
 #include <cuda_runtime.h>
