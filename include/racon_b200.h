@@ -154,6 +154,57 @@ int rb_poa_fetch(rb_ctx* ctx, rb_poa_result* out);
  * Results are identical to rb_poa_run's; fetch them with rb_poa_fetch. */
 int rb_poa_run_plain(rb_ctx* ctx);
 
+/* ---------------------------------------------------------------------
+ * Device layer assembly (replaces the layer loop of Polisher::initialize,
+ * src/polisher.cpp:384-457): the reads stay in device memory and the layers
+ * of every window are cut, filtered and ordered there.
+ * ------------------------------------------------------------------- */
+
+/* One entry of racon's sequence table: the targets first, then the reads that
+ * are not targets (src/polisher.cpp:209-281). data is uppercase; quality is
+ * NULL for FASTA input or when every value is '!' (racon drops it then).
+ * forward / reverse: whether some overlap uses the read on that strand
+ * (has_data / has_reverse_data of Sequence::transmute,
+ * src/polisher.cpp:355-372); targets set forward. Entries with neither are
+ * not copied. */
+typedef struct rb_sequence {
+    const char* data;
+    const char* quality;
+    uint32_t length;
+    uint8_t forward;
+    uint8_t reverse;
+} rb_sequence;
+
+/* Copies the sequence table to the device and builds the reverse complement
+ * and reversed quality (src/sequence.cpp:49-84) of every entry with reverse
+ * set. Replaces the previous table and drops windows staged from it. */
+int rb_sequences_stage(rb_ctx* ctx, const rb_sequence* sequences, size_t n);
+
+/* One overlap after find_overlap_breaking_points: read and target as indices
+ * into the staged table, strand 1 for '-'. */
+typedef struct rb_layer_overlap {
+    uint32_t q_id;
+    uint32_t t_id;
+    uint32_t strand;
+} rb_layer_overlap;
+
+/* Stages window consensus with the layers assembled on the device, as
+ * racon's initialize() assembles them (src/polisher.cpp:384-457): windows of
+ * rb_params.window_length bases over staged targets 0 .. n_targets-1, in
+ * racon's window order; overlap i's breaking points are
+ * breakpoints[bp_offsets[i] .. bp_offsets[i+1]) as (t, q) uint32 pairs, the
+ * layout of rb_aln_result (first match, last match + 1 per window). A pair
+ * becomes a layer of the window holding its first target position unless its
+ * query span is below 0.02 * window_length or, for a read with qualities, its
+ * mean Phred-33 quality is below quality_threshold; inside a window the
+ * layers keep overlap order and then take racon's sort by begin
+ * (src/window.cpp:78-85). tgs and trim as for rb_window / rb_poa_batch.
+ * Then rb_poa_run / rb_poa_run_plain / rb_poa_fetch (results in window
+ * order). The staged table must not change in between. */
+int rb_poa_stage_overlaps(rb_ctx* ctx, size_t n_targets, const rb_layer_overlap* overlaps, size_t n,
+                          const uint32_t* breakpoints, const uint64_t* bp_offsets, double quality_threshold,
+                          int tgs, int trim);
+
 /* Breaking points of overlaps that already carry an alignment (SAM input:
  * src/overlap.cpp:192-200 skips the aligner when the CIGAR is set and walks
  * it in find_breaking_points_from_cigar, :226-292). cigar is the SAM CIGAR
@@ -189,6 +240,11 @@ typedef struct rb_stats {
 } rb_stats;
 int rb_poa_stats(const rb_ctx* ctx, rb_stats* out);
 int rb_align_stats(const rb_ctx* ctx, rb_stats* out);
+/* Counters of the last rb_poa_stage_overlaps (kernel_ms: assembly kernels;
+ * items: layers kept; cells: breaking-point pairs examined) and of the last
+ * rb_sequences_stage (items: sequences; h2d: the store copy). */
+int rb_layer_stats(const rb_ctx* ctx, rb_stats* out);
+int rb_sequence_stats(const rb_ctx* ctx, rb_stats* out);
 
 /* ---------------------------------------------------------------------
  * Whole pipeline (createPolisher + initialize + polish, src/main.cpp:152-166)
@@ -220,6 +276,13 @@ rb_job* rb_job_prepare(const char* sequences_path, const char* overlaps_path,
                        double quality_threshold, double error_threshold, int8_t match,
                        int8_t mismatch, int8_t gap, int device, double* stage_seconds);
 size_t rb_job_windows(const rb_job* job, const rb_window** windows);
+/* The same job as device layer assembly input (rb_sequences_stage,
+ * rb_poa_stage_overlaps): its sequence table (targets first), the number of
+ * targets, the kept overlaps with their breaking points, and racon's window
+ * type (1 = kTGS). Views valid until rb_job_free. */
+int rb_job_layer_input(const rb_job* job, const rb_sequence** sequences, size_t* n_sequences, size_t* n_targets,
+                       const rb_layer_overlap** overlaps, size_t* n_overlaps, const uint32_t** breakpoints,
+                       const uint64_t** bp_offsets, int* tgs);
 void rb_job_free(rb_job* job);
 void rb_free(void* p);
 

@@ -68,6 +68,15 @@ class _Window(ctypes.Structure):
                 ("tgs", ctypes.c_uint8), ("id", ctypes.c_uint64), ("rank", ctypes.c_uint32)]
 
 
+class _Sequence(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("quality", ctypes.c_void_p), ("length", ctypes.c_uint32),
+                ("forward", ctypes.c_uint8), ("reverse", ctypes.c_uint8)]
+
+
+class _LayerOverlap(ctypes.Structure):
+    _fields_ = [("q_id", ctypes.c_uint32), ("t_id", ctypes.c_uint32), ("strand", ctypes.c_uint32)]
+
+
 class _PoaResult(ctypes.Structure):
     _fields_ = [("consensus", ctypes.POINTER(ctypes.c_char)), ("offsets", ctypes.POINTER(ctypes.c_uint64)),
                 ("polished", ctypes.POINTER(ctypes.c_uint8))]
@@ -130,6 +139,19 @@ def load():
     lib.rb_poa_run_plain.argtypes = [vp]
     lib.rb_poa_fetch.argtypes = [vp, ctypes.POINTER(_PoaResult)]
     lib.rb_poa_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    lib.rb_sequences_stage.argtypes = [vp, ctypes.POINTER(_Sequence), ctypes.c_size_t]
+    lib.rb_poa_stage_overlaps.argtypes = [vp, ctypes.c_size_t, ctypes.POINTER(_LayerOverlap), ctypes.c_size_t,
+                                          ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    lib.rb_layer_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    lib.rb_sequence_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    lib.rb_job_layer_input.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(_Sequence)),
+                                       ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+                                       ctypes.POINTER(ctypes.POINTER(_LayerOverlap)),
+                                       ctypes.POINTER(ctypes.c_size_t),
+                                       ctypes.POINTER(ctypes.POINTER(ctypes.c_uint32)),
+                                       ctypes.POINTER(ctypes.POINTER(ctypes.c_uint64)),
+                                       ctypes.POINTER(ctypes.c_int)]
     lib.rb_align_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.rb_polish_files.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
                                     ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_int,
@@ -316,6 +338,67 @@ class Context:
         self._check(self.lib.rb_poa_stage(self.ptr, job.windows, job.n, int(trim)))
         self._staged_windows = job.n
 
+    # ---- device layer assembly ----
+    def sequences_stage(self, sequences):
+        """sequences: racon's sequence table (targets first) as dicts with
+        data, quality (or None), forward, reverse (rb_sequences_stage)."""
+        n = len(sequences)
+        arr = (_Sequence * max(1, n))()
+        keep = []
+        for i, e in enumerate(sequences):
+            d = _b(e["data"]) or b""
+            q = _b(e.get("quality"))
+            db = ctypes.create_string_buffer(d, max(1, len(d)))
+            qb = ctypes.create_string_buffer(q, max(1, len(q))) if q is not None else None
+            keep += [db, qb]
+            arr[i] = _Sequence(ctypes.addressof(db), ctypes.addressof(qb) if qb is not None else None, len(d),
+                               int(e.get("forward", 1)), int(e.get("reverse", 0)))
+        self._check(self.lib.rb_sequences_stage(self.ptr, arr, n))
+        self._seq_lengths = [len(_b(e["data"]) or b"") for e in sequences]
+
+    def poa_stage_overlaps(self, n_targets, overlaps, quality_threshold=10.0, tgs=True, trim=True):
+        """overlaps: dicts with q_id, t_id, strand and breakpoints, a list of
+        (t, q) points (first match, last match + 1 per window). Stages the
+        consensus of every window over the first n_targets staged sequences
+        with the layers assembled on the device (rb_poa_stage_overlaps)."""
+        n = len(overlaps)
+        arr = (_LayerOverlap * max(1, n))()
+        flat, offs = [], [0]
+        for i, o in enumerate(overlaps):
+            arr[i] = _LayerOverlap(o["q_id"], o["t_id"], int(o.get("strand", 0)))
+            for t, q in o["breakpoints"]:
+                flat += [t, q]
+            offs.append(len(flat))
+        bp = (ctypes.c_uint32 * max(1, len(flat)))(*flat)
+        off = (ctypes.c_uint64 * len(offs))(*offs)
+        self._check(self.lib.rb_poa_stage_overlaps(self.ptr, n_targets, arr, n, bp, off, quality_threshold,
+                                                   int(tgs), int(trim)))
+        w = self.window_length
+        self._staged_windows = sum((n + w - 1) // w for n in self._seq_lengths[:n_targets])
+        return self._staged_windows
+
+    def poa_stage_job_device(self, job, trim=True, quality_threshold=None):
+        """Stages a Job's windows through the device layer assembly: its
+        sequence table to the device store, then its overlaps' breaking
+        points (host buffers, copies included)."""
+        inp = job.layer_input()
+        self._check(self.lib.rb_sequences_stage(self.ptr, inp["sequences"], inp["n_sequences"]))
+        q = job.quality_threshold if quality_threshold is None else quality_threshold
+        self._check(self.lib.rb_poa_stage_overlaps(self.ptr, inp["n_targets"], inp["overlaps"], inp["n_overlaps"],
+                                                   inp["breakpoints"], inp["bp_offsets"], q, inp["tgs"],
+                                                   int(trim)))
+        self._staged_windows = job.n
+
+    def layer_stats(self):
+        s = Stats()
+        self._check(self.lib.rb_layer_stats(self.ptr, ctypes.byref(s)))
+        return s
+
+    def sequence_stats(self):
+        s = Stats()
+        self._check(self.lib.rb_sequence_stats(self.ptr, ctypes.byref(s)))
+        return s
+
     def poa_stats(self):
         s = Stats()
         self._check(self.lib.rb_poa_stats(self.ptr, ctypes.byref(s)))
@@ -362,6 +445,7 @@ class Job:
         if not self.ptr:
             raise RaconB200Error(1, self.lib.rb_pipeline_error().decode())
         self.stage_seconds = list(st)
+        self.quality_threshold = quality_threshold
         wp = ctypes.POINTER(_Window)()
         self.n = self.lib.rb_job_windows(self.ptr, ctypes.byref(wp))
         self.windows = wp
@@ -394,6 +478,23 @@ class Job:
             ends.append(w.ends[j])
         return {"backbone": bb, "backbone_quality": bq, "layers": layers, "qualities": quals, "begins": begins,
                 "ends": ends, "tgs": w.tgs, "id": w.id, "rank": w.rank}
+
+    def layer_input(self):
+        """The job as device layer assembly input (rb_job_layer_input): ctypes
+        views of its sequence table, overlaps and breaking points."""
+        seqs = ctypes.POINTER(_Sequence)()
+        ovl = ctypes.POINTER(_LayerOverlap)()
+        bp = ctypes.POINTER(ctypes.c_uint32)()
+        off = ctypes.POINTER(ctypes.c_uint64)()
+        ns, nt, no = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
+        tgs = ctypes.c_int()
+        rc = self.lib.rb_job_layer_input(self.ptr, ctypes.byref(seqs), ctypes.byref(ns), ctypes.byref(nt),
+                                         ctypes.byref(ovl), ctypes.byref(no), ctypes.byref(bp), ctypes.byref(off),
+                                         ctypes.byref(tgs))
+        if rc != RB_OK:
+            raise RaconB200Error(rc, "rb_job_layer_input failed")
+        return {"sequences": seqs, "n_sequences": ns.value, "n_targets": nt.value, "overlaps": ovl,
+                "n_overlaps": no.value, "breakpoints": bp, "bp_offsets": off, "tgs": tgs.value}
 
     def layer_stats(self):
         """(windows, layers, layer bases, backbone bases)."""

@@ -8,7 +8,8 @@
 //   src/polisher.cpp:486-548  polish (stitching, tags, drop rule)
 // The two hot calls go to the device through include/racon_b200.h:
 //   find_overlap_breaking_points -> rb_align_batch / rb_cigar_breakpoints
-//   polish                      -> rb_poa_batch (window consensus)
+//   layer assembly              -> rb_sequences_stage + rb_poa_stage_overlaps
+//   polish                      -> rb_poa_run + rb_poa_fetch (window consensus)
 // Input readers (the reference uses the absent bioparser library) are
 // written here: FASTA/FASTQ (multi-line, gzip or plain), PAF, MHAP, SAM;
 // names end at the first whitespace.
@@ -285,7 +286,9 @@ void Sequence::create_reverse_complement() {
 void Sequence::transmute(bool has_name, bool has_data, bool has_reverse_data) {
     if (!has_name) std::string().swap(name_);
     if (has_reverse_data) create_reverse_complement();
-    if (!has_data) {
+    // the forward strand also stays when only the reverse one is used: the
+    // device builds its own reverse complement from it
+    if (!has_data && !has_reverse_data) {
         std::string().swap(data_);
         std::string().swap(quality_);
     }
@@ -701,37 +704,75 @@ void Polisher::initialize() {
         }
         first_window[i + 1] = first_window[i] + k;
     }
-    // layers (src/polisher.cpp:401-457)
+    // layers (src/polisher.cpp:401-457), assembled on the device from the
+    // overlaps' ids, strands and breaking points
     targets_coverages_.assign(targets_size, 0);
+    layer_overlaps_.clear();
+    breakpoints_.clear();
+    bp_offsets_.assign(1, 0);
     for (auto& o : overlaps) {
         ++targets_coverages_[o->t_id];
-        const Sequence& s = *sequences_[o->q_id];
-        const auto& bp = o->breaking_points;
+        layer_overlaps_.push_back(rb_layer_overlap{uint32_t(o->q_id), uint32_t(o->t_id), o->strand ? 1u : 0u});
+        for (const auto& p : o->breaking_points) {
+            breakpoints_.push_back(p.first);
+            breakpoints_.push_back(p.second);
+        }
+        bp_offsets_.push_back(breakpoints_.size());
+        o.reset();
+    }
+    sequence_table_.resize(sequences_.size());
+    for (size_t i = 0; i < sequences_.size(); ++i) {
+        const Sequence& q = *sequences_[i];
+        rb_sequence& e = sequence_table_[i];
+        e.data = q.data().data();
+        e.quality = q.quality().empty() ? nullptr : q.quality().data();
+        e.length = uint32_t(q.data().size());
+        e.forward = has_data[i] ? 1 : 0;
+        e.reverse = has_reverse[i] ? 1 : 0;
+    }
+    if (rb_sequences_stage(ctx_, sequence_table_.data(), sequence_table_.size()) != RB_OK ||
+        rb_poa_stage_overlaps(ctx_, targets_size, layer_overlaps_.data(), layer_overlaps_.size(),
+                              breakpoints_.data(), bp_offsets_.data(), quality_threshold_, tgs_ ? 1 : 0,
+                              trim_ ? 1 : 0) != RB_OK)
+        fail(std::string("[racon::Polisher::initialize] error: ") + rb_last_error(ctx_));
+    staged_ = true;
+    const double t3 = now_s();
+    stage_s_[0] = t1 - t0;
+    stage_s_[1] = t2 - t1;
+    stage_s_[2] = t3 - t2;
+}
+
+void Polisher::assemble_host_layers() {
+    const size_t targets_size = targets_coverages_.size();
+    std::vector<uint64_t> first_window(targets_size + 1, 0);
+    for (const auto& w : windows_) ++first_window[w->id + 1];
+    for (size_t i = 0; i < targets_size; ++i) first_window[i + 1] += first_window[i];
+    for (size_t i = 0; i < layer_overlaps_.size(); ++i) {
+        const rb_layer_overlap& o = layer_overlaps_[i];
+        const Sequence& s = *sequences_[o.q_id];
+        std::vector<std::pair<uint32_t, uint32_t>> bp;
+        for (uint64_t x = bp_offsets_[i]; x < bp_offsets_[i + 1]; x += 2)
+            bp.emplace_back(breakpoints_[x], breakpoints_[x + 1]);
         for (size_t j = 0; j + 1 < bp.size(); j += 2) {
             if (bp[j + 1].second - bp[j].second < 0.02 * window_length_) continue;
             if (!s.quality().empty() || !s.reverse_quality().empty()) {
-                const std::string& q = o->strand ? s.reverse_quality() : s.quality();
+                const std::string& q = o.strand ? s.reverse_quality() : s.quality();
                 double avg = 0;
                 for (uint32_t k = bp[j].second; k < bp[j + 1].second; ++k) avg += static_cast<uint32_t>(q[k]) - 33;
                 avg /= bp[j + 1].second - bp[j].second;
                 if (avg < quality_threshold_) continue;
             }
-            const uint64_t wid = first_window[o->t_id] + bp[j].first / window_length_;
+            const uint64_t wid = first_window[o.t_id] + bp[j].first / window_length_;
             const uint32_t wstart = (bp[j].first / window_length_) * window_length_;
-            const char* data = o->strand ? &s.reverse_complement()[bp[j].second] : &s.data()[bp[j].second];
+            const char* data = o.strand ? &s.reverse_complement()[bp[j].second] : &s.data()[bp[j].second];
             const uint32_t dlen = bp[j + 1].second - bp[j].second;
-            const char* qual = o->strand
+            const char* qual = o.strand
                                    ? (s.reverse_quality().empty() ? nullptr : &s.reverse_quality()[bp[j].second])
                                    : (s.quality().empty() ? nullptr : &s.quality()[bp[j].second]);
             windows_[wid]->add_layer(data, dlen, qual, qual ? dlen : 0, bp[j].first - wstart,
                                      bp[j + 1].first - wstart - 1);
         }
-        o.reset();
     }
-    const double t3 = now_s();
-    stage_s_[0] = t1 - t0;
-    stage_s_[1] = t2 - t1;
-    stage_s_[2] = t3 - t2;
 }
 
 // Device alignment of every overlap without a CIGAR, device CIGAR walk for
@@ -806,34 +847,15 @@ void Polisher::polish(std::vector<std::unique_ptr<Sequence>>& dst, bool drop_unp
     const double t0 = now_s();
     const size_t nw = windows_.size();
     std::vector<uint8_t> polished(nw, 0);
-    // device consensus in batches of windows
-    const size_t kBatch = 65536;
-    for (size_t b = 0; b < nw; b += kBatch) {
-        const size_t e = std::min(nw, b + kBatch);
-        std::vector<rb_window> wins(e - b);
-        for (size_t i = b; i < e; ++i) {
-            const Window& w = *windows_[i];
-            rb_window& r = wins[i - b];
-            r.backbone = w.backbone;
-            r.backbone_quality = w.quality;
-            r.backbone_length = w.backbone_length;
-            r.n_layers = uint32_t(w.seqs.size());
-            r.layers = w.seqs.data();
-            r.layer_qualities = w.quals.data();
-            r.layer_lengths = w.lens.data();
-            r.begins = w.begins.data();
-            r.ends = w.ends.data();
-            r.tgs = tgs_ ? 1 : 0;
-            r.id = w.id;
-            r.rank = w.rank;
-        }
-        rb_poa_result r;
-        if (rb_poa_batch(ctx_, wins.data(), wins.size(), trim_ ? 1 : 0, &r) != RB_OK)
-            fail(std::string("[racon::Polisher::polish] error: ") + rb_last_error(ctx_));
-        for (size_t i = b; i < e; ++i) {
-            windows_[i]->consensus.assign(r.consensus + r.offsets[i - b], r.consensus + r.offsets[i - b + 1]);
-            polished[i] = r.polished[i - b];
-        }
+    // device consensus of the windows initialize() staged
+    if (!staged_) fail("[racon::Polisher::polish] error: windows are not staged (initialize first)");
+    rb_poa_result r;
+    if (rb_poa_run(ctx_) != RB_OK || rb_poa_fetch(ctx_, &r) != RB_OK)
+        fail(std::string("[racon::Polisher::polish] error: ") + rb_last_error(ctx_));
+    staged_ = false;
+    for (size_t i = 0; i < nw; ++i) {
+        windows_[i]->consensus.assign(r.consensus + r.offsets[i], r.consensus + r.offsets[i + 1]);
+        polished[i] = r.polished[i];
     }
     // stitching (src/polisher.cpp:506-533)
     std::string data;
@@ -967,8 +989,10 @@ struct rb_job {
     std::vector<rb_window> views;
     double stage_s[3] = {0, 0, 0};
 
-    // window views after initialize() (friend of racon::Polisher)
+    // window views after initialize() (friend of racon::Polisher); the
+    // layers are assembled on the host for them
     void collect() {
+        polisher->assemble_host_layers();
         const racon::Polisher& p = *polisher;
         views.resize(p.windows_.size());
         for (size_t i = 0; i < p.windows_.size(); ++i) {
@@ -1022,6 +1046,24 @@ extern "C" size_t rb_job_windows(const rb_job* job, const rb_window** windows) {
     if (!job || !windows) return 0;
     *windows = job->views.data();
     return job->views.size();
+}
+
+extern "C" int rb_job_layer_input(const rb_job* job, const rb_sequence** sequences, size_t* n_sequences,
+                                  size_t* n_targets, const rb_layer_overlap** overlaps, size_t* n_overlaps,
+                                  const uint32_t** breakpoints, const uint64_t** bp_offsets, int* tgs) {
+    if (!job || !sequences || !n_sequences || !n_targets || !overlaps || !n_overlaps || !breakpoints ||
+        !bp_offsets || !tgs)
+        return RB_ERR_ARG;
+    const racon::Polisher& p = *job->polisher;
+    *sequences = p.sequence_table_.data();
+    *n_sequences = p.sequence_table_.size();
+    *n_targets = p.targets_coverages_.size();
+    *overlaps = p.layer_overlaps_.data();
+    *n_overlaps = p.layer_overlaps_.size();
+    *breakpoints = p.breakpoints_.data();
+    *bp_offsets = p.bp_offsets_.data();
+    *tgs = p.tgs_ ? 1 : 0;
+    return RB_OK;
 }
 
 extern "C" void rb_job_free(rb_job* job) { delete job; }

@@ -17,7 +17,8 @@
 #include <utility>
 #include <vector>
 
-struct rb_ctx;
+#include "../../../include/racon_b200.h"
+
 struct rb_job;
 
 namespace racon {
@@ -90,6 +91,8 @@ public:
         uint32_t num_threads, uint32_t cuda_batches, bool cuda_banded_alignment,
         uint32_t cudaaligner_batches, uint32_t cudaaligner_band_width);
     friend struct ::rb_job;
+    friend int ::rb_job_layer_input(const rb_job*, const rb_sequence**, size_t*, size_t*,
+                                    const rb_layer_overlap**, size_t*, const uint32_t**, const uint64_t**, int*);
     friend std::unique_ptr<Polisher> createPolisherOnContext(rb_ctx* ctx, int device,
         const std::string& sequences_path, const std::string& overlaps_path,
         const std::string& target_path, PolisherType type, uint32_t window_length,
@@ -106,6 +109,10 @@ protected:
     Polisher(const Polisher&) = delete;
     const Polisher& operator=(const Polisher&) = delete;
     virtual void find_overlap_breaking_points(std::vector<std::unique_ptr<Overlap>>& overlaps);
+    // Window layers on the host from the kept overlaps (the loop of
+    // src/polisher.cpp:401-457), for callers that want rb_window views; the
+    // polishing path assembles them on the device instead.
+    void assemble_host_layers();
 
     std::string sequences_path_, overlaps_path_, target_path_;
     int sequences_format_, overlaps_format_, target_format_;
@@ -123,6 +130,15 @@ protected:
     uint32_t window_length_;
     std::vector<std::shared_ptr<Window>> windows_;
     bool tgs_ = true;
+
+    // input of the device layer assembly (rb_sequences_stage,
+    // rb_poa_stage_overlaps): the sequence table with the strands the
+    // overlaps use, and each kept overlap's ids, strand and breaking points
+    std::vector<rb_sequence> sequence_table_;
+    std::vector<rb_layer_overlap> layer_overlaps_;
+    std::vector<uint32_t> breakpoints_;
+    std::vector<uint64_t> bp_offsets_;
+    bool staged_ = false;
 
     uint32_t num_threads_;
     int device_ = 0;

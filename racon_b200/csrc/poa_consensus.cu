@@ -44,7 +44,6 @@ namespace {
 
 // minus infinity that survives thousands of gap additions without overflow
 constexpr int kNegInf = -(1 << 29);
-constexpr uint64_t kNoQual = ~0ull;
 // per-warp shared memory: the DP row ring, reused by the other steps
 constexpr int kRingBytesPerWarp = 16384;
 // node ranks held in the ring's shared memory during the descriptor build
@@ -55,25 +54,6 @@ enum PoaFlag : uint8_t {
     kChimeric = 2,
     kOverflow = 4,
     kFailed = 8,
-};
-
-struct PoaWinDev {
-    uint64_t bb_off;
-    uint64_t bq_off;       // kNoQual: weight 0 ('!' dummy quality)
-    uint64_t layer_base;   // first entry in the layer table (already in racon's sorted order)
-    uint64_t out_off;
-    uint32_t bb_len;
-    uint32_t n_layers;
-    uint32_t out_cap;
-    uint32_t offset;       // uint32(0.01 * backbone length)
-    uint32_t tgs;
-    uint32_t pad;
-};
-
-struct PoaLayerDev {
-    uint64_t seq_off;
-    uint64_t qual_off;     // kNoQual: weight 1 per base
-    uint32_t len, begin, end, pad;
 };
 
 struct PoaArgs {
@@ -2394,9 +2374,17 @@ PoaEngine::~PoaEngine() {
     cudaEventDestroy(ev3_);
 }
 
+// Phred+33 bytes '!'..'~': the window graph weights are quality - 33 in
+// 0..93 (spoa's uint32 weights of other bytes are not modelled).
+static bool phred_bytes(const char* q, uint32_t n) {
+    uint8_t bad = 0;
+    for (uint32_t k = 0; k < n; ++k) bad |= uint8_t(uint8_t(q[k] - 33) > 93);
+    return bad == 0;
+}
+
 void PoaEngine::stage(const rb_window* wins, size_t n, int trim) {
     if (n > 0 && !wins) throw Error{RB_ERR_ARG, "rb_poa: windows is NULL"};
-    nwin_ = n;
+    forget();
     trim_ = trim;
     // sizes
     uint64_t in_bytes = 0, nlayers = 0, out_cap = 0;
@@ -2449,6 +2437,8 @@ void PoaEngine::stage(const rb_window* wins, size_t n, int trim) {
         memcpy(in + off, w.backbone, w.backbone_length);
         off += (w.backbone_length + 15) & ~15u;
         if (w.backbone_quality) {
+            if (!phred_bytes(w.backbone_quality, w.backbone_length))
+                throw Error{RB_ERR_ARG, "rb_poa: quality values outside '!'..'~' (Phred+33 0..93)"};
             d.bq_off = off;
             memcpy(in + off, w.backbone_quality, w.backbone_length);
             off += (w.backbone_length + 15) & ~15u;
@@ -2483,6 +2473,8 @@ void PoaEngine::stage(const rb_window* wins, size_t n, int trim) {
             off += (l + 15) & ~15u;
             const char* q = w.layer_qualities ? w.layer_qualities[s] : nullptr;
             if (q) {
+                if (!phred_bytes(q, l))
+                    throw Error{RB_ERR_ARG, "rb_poa: quality values outside '!'..'~' (Phred+33 0..93)"};
                 L.qual_off = off;
                 memcpy(in + off, q, l);
                 off += (l + 15) & ~15u;
@@ -2524,6 +2516,60 @@ void PoaEngine::stage(const rb_window* wins, size_t n, int trim) {
     stats_.h2d_ms = ms;
     stats_.h2d_bytes = off + n * (sizeof(PoaWinDev) + 4) + nlayers * sizeof(PoaLayerDev);
     in_bytes_ = off;
+    in_ptr_ = d_in_.as<uint8_t>();
+    layers_ptr_ = d_layers_.as<PoaLayerDev>();
+    nwin_ = n;
+}
+
+void PoaEngine::stage_device(const uint8_t* d_in, const PoaWinDev* wins, size_t n, const PoaLayerDev* d_layers,
+                             const uint64_t* sum_len, const std::vector<std::pair<uint64_t, uint32_t>>& labels,
+                             uint32_t max_len, int trim) {
+    forget();
+    trim_ = trim;
+    max_len_ = max_len;
+    uint64_t out_cap = 0;
+    uint32_t max_nodes = 0;
+    for (size_t i = 0; i < n; ++i) {
+        out_cap = std::max<uint64_t>(out_cap, wins[i].out_off + wins[i].out_cap);
+        max_nodes = uint32_t(std::max<uint64_t>(max_nodes, std::min<uint64_t>(wins[i].bb_len + sum_len[i], 1u << 20)));
+    }
+    out_cap_ = out_cap;
+    max_nodes_cap_ = max_nodes;
+    labels_.assign(labels.begin(), labels.begin() + n);
+    h_desc_.reserve(std::max<size_t>(n, 1) * sizeof(PoaWinDev));
+    h_order_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
+    PoaWinDev* wd = h_desc_.as<PoaWinDev>();
+    if (n) memcpy(wd, wins, n * sizeof(PoaWinDev));
+    // size-sorted queue, the same work estimate as stage()
+    uint32_t* order = h_order_.as<uint32_t>();
+    std::iota(order, order + n, 0u);
+    std::vector<uint64_t> work(n);
+    for (size_t i = 0; i < n; ++i) {
+        const uint64_t s = sum_len[i];
+        work[i] = s * (wd[i].bb_len + s / std::max<uint32_t>(1, wd[i].n_layers));
+    }
+    std::sort(order, order + n, [&](uint32_t x, uint32_t y) { return work[x] != work[y] ? work[x] > work[y] : x < y; });
+    d_desc_.reserve(std::max<size_t>(n, 1) * sizeof(PoaWinDev));
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    if (n)
+        check_cuda(cudaMemcpyAsync(d_desc_.ptr, wd, n * sizeof(PoaWinDev), cudaMemcpyHostToDevice, stream_),
+                   "H2D desc");
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    check_cuda(cudaStreamSynchronize(stream_), "stage sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.h2d_ms = ms;
+    stats_.h2d_bytes = n * sizeof(PoaWinDev);
+    in_bytes_ = 0;
+    in_ptr_ = d_in;
+    layers_ptr_ = d_layers;
+    nwin_ = n;
+}
+
+void PoaEngine::forget() {
+    nwin_ = 0;
+    in_ptr_ = nullptr;
+    layers_ptr_ = nullptr;
 }
 
 void PoaEngine::run(bool plain) {
@@ -2571,9 +2617,9 @@ void PoaEngine::run(bool plain) {
                    "H2D todo");
         PoaArgs a;
         memset(&a, 0, sizeof(a));
-        a.in = d_in_.as<uint8_t>();
+        a.in = in_ptr_;
         a.wins = d_desc_.as<PoaWinDev>();
-        a.layers = d_layers_.as<PoaLayerDev>();
+        a.layers = layers_ptr_;
         a.order = d_todo.as<uint32_t>();
         a.nwin = uint32_t(todo.size());
         a.out = d_out_.as<char>();

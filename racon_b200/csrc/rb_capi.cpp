@@ -54,6 +54,7 @@ struct rb_ctx {
     rb_params params{};
     std::unique_ptr<rb::NwEngine> nw;
     std::unique_ptr<rb::PoaEngine> poa;
+    std::unique_ptr<rb::LayerEngine> layers;
     std::string err;
 };
 
@@ -133,6 +134,7 @@ rb_ctx* rb_create(int device, const rb_params* params) {
         rb::check_cuda(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         ctx->nw.reset(new rb::NwEngine(ctx->dev, ctx->stream));
         ctx->poa.reset(new rb::PoaEngine(ctx->dev, ctx->stream, params->match, params->mismatch, params->gap));
+        ctx->layers.reset(new rb::LayerEngine(ctx->dev, ctx->stream));
     } catch (const rb::Error& e) {
         set_create_error(e.msg);
         return nullptr;
@@ -149,6 +151,7 @@ void rb_destroy(rb_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->dev.device);
     ctx->nw.reset();
+    ctx->layers.reset();
     ctx->poa.reset();
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -201,6 +204,28 @@ int rb_poa_batch(rb_ctx* ctx, const rb_window* windows, size_t n, int trim, rb_p
         ctx->poa->run();
         ctx->poa->fetch(out);
     });
+}
+
+int rb_sequences_stage(rb_ctx* ctx, const rb_sequence* sequences, size_t n) {
+    return guarded(ctx, [&]() { ctx->layers->stage_sequences(sequences, n, *ctx->poa); });
+}
+int rb_poa_stage_overlaps(rb_ctx* ctx, size_t n_targets, const rb_layer_overlap* overlaps, size_t n,
+                          const uint32_t* breakpoints, const uint64_t* bp_offsets, double quality_threshold,
+                          int tgs, int trim) {
+    return guarded(ctx, [&]() {
+        ctx->layers->assemble(n_targets, overlaps, n, breakpoints, bp_offsets, ctx->params.window_length,
+                              quality_threshold, tgs, trim, *ctx->poa);
+    });
+}
+int rb_layer_stats(const rb_ctx* ctx, rb_stats* out) {
+    if (!ctx || !out) return RB_ERR_ARG;
+    *out = ctx->layers->stats();
+    return RB_OK;
+}
+int rb_sequence_stats(const rb_ctx* ctx, rb_stats* out) {
+    if (!ctx || !out) return RB_ERR_ARG;
+    *out = ctx->layers->sequence_stats();
+    return RB_OK;
 }
 
 int rb_poa_stats(const rb_ctx* ctx, rb_stats* out) {

@@ -92,11 +92,45 @@ private:
 };
 
 // ----- window consensus engine (poa_consensus.cu) -----
+// Device records of a staged batch: windows and their layers, byte offsets
+// into one input buffer (packed by PoaEngine::stage, or the resident
+// sequence store of LayerEngine).
+constexpr uint64_t kNoQual = ~0ull;
+
+struct PoaWinDev {
+    uint64_t bb_off;
+    uint64_t bq_off;       // kNoQual: weight 0 ('!' dummy quality)
+    uint64_t layer_base;   // first entry in the layer table (already in racon's sorted order)
+    uint64_t out_off;
+    uint32_t bb_len;
+    uint32_t n_layers;
+    uint32_t out_cap;
+    uint32_t offset;       // uint32(0.01 * backbone length)
+    uint32_t tgs;
+    uint32_t pad;
+};
+
+struct PoaLayerDev {
+    uint64_t seq_off;
+    uint64_t qual_off;     // kNoQual: weight 1 per base
+    uint32_t len, begin, end, pad;
+};
+
 class PoaEngine {
 public:
     PoaEngine(const DeviceInfo& dev, cudaStream_t stream, int8_t m, int8_t x, int8_t g);
     ~PoaEngine();
     void stage(const rb_window* wins, size_t n, int trim);
+    // Windows whose bytes and layer records already sit in device memory
+    // (device layer assembly): d_in holds every offset of wins and of the
+    // d_layers records; sum_len[i] is the total layer length of window i and
+    // labels[i] its (target id, rank). The device buffers must stay
+    // unchanged until the next stage call or forget().
+    void stage_device(const uint8_t* d_in, const PoaWinDev* wins, size_t n, const PoaLayerDev* d_layers,
+                      const uint64_t* sum_len, const std::vector<std::pair<uint64_t, uint32_t>>& labels,
+                      uint32_t max_len, int trim);
+    // Drops a device stage whose buffers are about to change.
+    void forget();
     void run(bool plain = false);
     void fetch(rb_poa_result* out);
     const rb_stats& stats() const { return stats_; }
@@ -115,6 +149,8 @@ private:
     size_t nwin_ = 0;
     uint64_t in_bytes_ = 0, out_cap_ = 0;
     uint32_t max_len_ = 0, max_nodes_cap_ = 0;
+    const uint8_t* in_ptr_ = nullptr;          // input bytes of the staged windows
+    const PoaLayerDev* layers_ptr_ = nullptr;  // their layer records
     HostBuf h_in_, h_desc_, h_layers_, h_order_, h_out_, h_outlen_, h_flags_;
     DevBuf d_in_, d_desc_, d_layers_, d_order_, d_out_, d_outlen_, d_flags_, d_misc_;
     DevBuf d_graph_, d_dp_;
@@ -125,6 +161,48 @@ private:
     std::vector<std::pair<uint64_t, uint32_t>> labels_;  // (id, rank) per window
     size_t scratch_budget_ = size_t(48) << 30;
     rb_stats stats_{};
+};
+
+// ----- device layer assembly (layers.cu) -----
+class LayerEngine {
+public:
+    LayerEngine(const DeviceInfo& dev, cudaStream_t stream);
+    ~LayerEngine();
+    // Copies the sequence table to the device store and builds the reverse
+    // complements there; drops any window stage of poa that reads the store.
+    void stage_sequences(const rb_sequence* seqs, size_t n, PoaEngine& poa);
+    // Layers of every window over targets 0 .. n_targets-1 from host
+    // breaking points, then poa.stage_device.
+    void assemble(size_t n_targets, const rb_layer_overlap* ovl, size_t n, const uint32_t* bps,
+                  const uint64_t* bp_offsets, uint32_t window_length, double quality_threshold, int tgs, int trim,
+                  PoaEngine& poa);
+    const rb_stats& stats() const { return stats_; }
+    const rb_stats& sequence_stats() const { return seq_stats_; }
+
+private:
+    void begin(size_t n_targets, uint32_t window_length, double quality_threshold, uint64_t cand_cap);
+    void add_candidates(const uint32_t* d_bp, const uint32_t* d_bpcnt, const void* d_ovl, size_t n);
+    void finish(int tgs, int trim, PoaEngine& poa);
+    uint32_t* win_cnt() const;
+    uint32_t* win_fill() const;
+    uint64_t* win_base() const;
+    unsigned long long* win_sum() const;
+    uint32_t* status() const;
+
+    DeviceInfo dev_;
+    cudaStream_t stream_;
+    cudaEvent_t ev0_, ev1_;
+    size_t nseq_ = 0, n_targets_ = 0;
+    uint64_t nwin_ = 0, cand_cap_ = 0, store_bytes_ = 0;
+    uint32_t w_ = 500;
+    double q_threshold_ = 10.0;
+    int batches_ = 0;
+    float cand_ms_ = 0;
+    std::vector<uint32_t> lens_;
+    std::vector<uint64_t> fwd_, fq_, first_window_;
+    HostBuf h_store_, h_misc_, h_bp_, h_fw_, h_lay_, h_perm_;
+    DevBuf d_store_, d_seqs_, d_list_, d_bp_, d_ovl_, d_fw_, d_cand_, d_cand_win_, d_win_, d_lay_, d_final_;
+    rb_stats stats_{}, seq_stats_{};
 };
 
 // Caps the window-consensus scratch of a context (server workers share one
