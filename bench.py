@@ -10,8 +10,12 @@ untimed; a step is the consensus of every window of the job.
 
   value  windows/s with the windows staged in HBM (rb_poa_run), device time
          from CUDA events on the library's stream, max over ranks
-  e2e    windows/s through the C ABI with host buffers (rb_poa_batch: pack,
-         H2D, kernels, D2H, unpack) per step, wall time
+  e2e    windows/s through the C ABI with host buffers, wall time per step:
+         the polishing path's own calls (rb_sequences_stage: sequence table
+         to the device; rb_poa_stage_overlaps: layers assembled on the
+         device from the breaking points; rb_poa_run; rb_poa_fetch)
+  e2e_host_layers  the same through rb_poa_batch with host-assembled
+         windows (pack every layer's bases, H2D, kernels, D2H, unpack)
   roofline / compute  see DESIGN.md (the POA DP is integer-issue bound)
   cpu_baseline  the CPU oracle (restatement of racon's algorithm, not
          reference racon, which does not build here) on a bounded sample of
@@ -542,21 +546,46 @@ def main():
     t_max = max_over_ranks(sum(plain_ms) / 1000.0, world)
     plain_value = world * n_win * args.steps / t_max
 
-    # ---- end to end through the C ABI with host buffers ----
-    for _ in range(1):
-        ctx.poa_job(job)
+    # ---- end to end through the C ABI with host buffers: the polishing
+    # path (sequence table + breaking points in, layers assembled on the
+    # device) ----
+    def device_step():
+        ctx.poa_stage_job_device(job)
+        ctx.poa_run()
+        res = ctx.poa_fetch()
+        sq, ly, po = ctx.sequence_stats(), ctx.layer_stats(), ctx.poa_stats()
+        return res, sq.h2d_bytes + ly.h2d_bytes + po.h2d_bytes, ly.d2h_bytes + po.d2h_bytes, ly
+
+    device_step()
     barrier()
     t0 = time.perf_counter()
     h2d = d2h = 0
+    layer_ms, layer_launches = [], 0
     for _ in range(args.steps):
-        res = ctx.poa_job(job)
-        st = ctx.poa_stats()
-        h2d += st.h2d_bytes
-        d2h += st.d2h_bytes
+        res, hb, db, ly = device_step()
+        h2d += hb
+        d2h += db
+        layer_ms.append(ly.kernel_ms)
+        layer_launches += ly.launches
     barrier()
     e2e_s = time.perf_counter() - t0
     t_max = max_over_ranks(e2e_s, world)
     e2e_value = world * n_win * args.steps / t_max
+    assert res == reference_out, "device layer assembly changed the consensus"
+
+    # ---- the same through rb_poa_batch with host-assembled windows ----
+    ctx.poa_job(job)
+    barrier()
+    t0 = time.perf_counter()
+    hh2d = hd2h = 0
+    for _ in range(args.steps):
+        res = ctx.poa_job(job)
+        st = ctx.poa_stats()
+        hh2d += st.h2d_bytes
+        hd2h += st.d2h_bytes
+    barrier()
+    t_max = max_over_ranks(time.perf_counter() - t0, world)
+    host_layers_value = world * n_win * args.steps / t_max
     assert res == reference_out
 
     # ---- roofline of the dominant kernel (poa_kernel) ----
@@ -585,7 +614,15 @@ def main():
                           "same per-window code, identical output (checked)"},
         "batched_vs_plain": value / plain_value,
         "e2e": {"value": e2e_value, "unit": "windows/s", "h2d_bytes_per_step": h2d // max(1, args.steps),
-                "d2h_bytes_per_step": d2h // max(1, args.steps)},
+                "d2h_bytes_per_step": d2h // max(1, args.steps),
+                "path": "rb_sequences_stage + rb_poa_stage_overlaps (device layer assembly) + rb_poa_run + "
+                        "rb_poa_fetch"},
+        "e2e_host_layers": {"value": host_layers_value, "unit": "windows/s",
+                            "h2d_bytes_per_step": hh2d // max(1, args.steps),
+                            "d2h_bytes_per_step": hd2h // max(1, args.steps),
+                            "path": "rb_poa_batch with host-assembled windows"},
+        "layer_assembly": {"kernel_ms_per_step": sum(layer_ms) / max(1, len(layer_ms)),
+                           "launches_per_step": layer_launches // max(1, args.steps), "layers": n_layers},
         "roofline": {"bound": "hbm", "kernel": "poa_kernel", "achieved": achieved_gbs,
                      "peak": peaks.get("hbm_gbs", 6650.0), "unit": "GB/s",
                      "frac": achieved_gbs / peaks.get("hbm_gbs", 6650.0),

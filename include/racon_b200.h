@@ -188,6 +188,34 @@ typedef struct rb_layer_overlap {
     uint32_t strand;
 } rb_layer_overlap;
 
+/* One overlap as racon's Overlap holds it, for alignment from the staged
+ * table: read q_id span [q_begin, q_end) and target t_id span
+ * [t_begin, t_end) in forward coordinates, strand 1 for '-'. The query is the
+ * read span, reverse-complemented for '-' (the span
+ * [length - q_end, length - q_begin) of the reverse complement,
+ * src/overlap.cpp:193-197); the target is the contig span. */
+typedef struct rb_store_pair {
+    uint32_t q_id;
+    uint32_t q_begin, q_end;
+    uint32_t t_id;
+    uint32_t t_begin, t_end;
+    uint32_t strand;
+} rb_store_pair;
+
+/* rb_align_stage for pairs cut from the staged table on the device (no
+ * sequence bytes cross the bus); then rb_align_run / rb_align_fetch as for
+ * rb_align_stage. Results equal rb_align_batch's on the same spans. */
+int rb_align_stage_overlaps(rb_ctx* ctx, const rb_store_pair* pairs, size_t n, int want_cigar);
+
+/* find_overlap_breaking_points and the layer assembly in one call
+ * (src/polisher.cpp:462-484 then :384-457): aligns every pair from the staged
+ * table, turns the breaking points into layers without leaving the device,
+ * and stages window consensus as rb_poa_stage_overlaps does. breakpoints may
+ * be NULL; otherwise it receives every pair's edit distance and breaking
+ * points (no CIGARs), library-owned until the next call on ctx. */
+int rb_poa_stage_alignments(rb_ctx* ctx, size_t n_targets, const rb_store_pair* pairs, size_t n,
+                            double quality_threshold, int tgs, int trim, rb_aln_result* breakpoints);
+
 /* Stages window consensus with the layers assembled on the device, as
  * racon's initialize() assembles them (src/polisher.cpp:384-457): windows of
  * rb_params.window_length bases over staged targets 0 .. n_targets-1, in

@@ -77,6 +77,12 @@ class _LayerOverlap(ctypes.Structure):
     _fields_ = [("q_id", ctypes.c_uint32), ("t_id", ctypes.c_uint32), ("strand", ctypes.c_uint32)]
 
 
+class _StorePair(ctypes.Structure):
+    _fields_ = [("q_id", ctypes.c_uint32), ("q_begin", ctypes.c_uint32), ("q_end", ctypes.c_uint32),
+                ("t_id", ctypes.c_uint32), ("t_begin", ctypes.c_uint32), ("t_end", ctypes.c_uint32),
+                ("strand", ctypes.c_uint32)]
+
+
 class _PoaResult(ctypes.Structure):
     _fields_ = [("consensus", ctypes.POINTER(ctypes.c_char)), ("offsets", ctypes.POINTER(ctypes.c_uint64)),
                 ("polished", ctypes.POINTER(ctypes.c_uint8))]
@@ -143,6 +149,10 @@ def load():
     lib.rb_poa_stage_overlaps.argtypes = [vp, ctypes.c_size_t, ctypes.POINTER(_LayerOverlap), ctypes.c_size_t,
                                           ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
                                           ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    lib.rb_align_stage_overlaps.argtypes = [vp, ctypes.POINTER(_StorePair), ctypes.c_size_t, ctypes.c_int]
+    lib.rb_poa_stage_alignments.argtypes = [vp, ctypes.c_size_t, ctypes.POINTER(_StorePair), ctypes.c_size_t,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(_AlnResult)]
     lib.rb_layer_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.rb_sequence_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.rb_job_layer_input.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(_Sequence)),
@@ -376,6 +386,37 @@ class Context:
         w = self.window_length
         self._staged_windows = sum((n + w - 1) // w for n in self._seq_lengths[:n_targets])
         return self._staged_windows
+
+    @staticmethod
+    def _store_pairs(pairs):
+        arr = (_StorePair * max(1, len(pairs)))()
+        for i, p in enumerate(pairs):
+            arr[i] = _StorePair(p["q_id"], p["q_begin"], p["q_end"], p["t_id"], p["t_begin"], p["t_end"],
+                                int(p.get("strand", 0)))
+        return arr
+
+    def align_overlaps(self, pairs, want_cigar=True):
+        """Aligns pairs cut from the staged sequence table (dicts with q_id,
+        q_begin, q_end, t_id, t_begin, t_end, strand; forward coordinates):
+        rb_align_stage_overlaps + rb_align_run + rb_align_fetch."""
+        arr = self._store_pairs(pairs)
+        self._check(self.lib.rb_align_stage_overlaps(self.ptr, arr, len(pairs), int(want_cigar)))
+        self._check(self.lib.rb_align_run(self.ptr))
+        r = _AlnResult()
+        self._check(self.lib.rb_align_fetch(self.ptr, ctypes.byref(r)))
+        return self._aln_out(r, len(pairs), want_cigar)
+
+    def poa_stage_alignments(self, n_targets, pairs, quality_threshold=10.0, tgs=True, trim=True):
+        """Aligns the pairs from the staged table and stages window consensus
+        with their breaking points turned into layers on the device
+        (rb_poa_stage_alignments). Returns [(edit distance, breakpoints)]."""
+        arr = self._store_pairs(pairs)
+        r = _AlnResult()
+        self._check(self.lib.rb_poa_stage_alignments(self.ptr, n_targets, arr, len(pairs), quality_threshold,
+                                                     int(tgs), int(trim), ctypes.byref(r)))
+        w = self.window_length
+        self._staged_windows = sum((n + w - 1) // w for n in self._seq_lengths[:n_targets])
+        return [(x["edit_distance"], x["breakpoints"]) for x in self._aln_out(r, len(pairs), False)]
 
     def poa_stage_job_device(self, job, trim=True, quality_threshold=None):
         """Stages a Job's windows through the device layer assembly: its

@@ -285,9 +285,9 @@ void Sequence::create_reverse_complement() {
 
 void Sequence::transmute(bool has_name, bool has_data, bool has_reverse_data) {
     if (!has_name) std::string().swap(name_);
-    if (has_reverse_data) create_reverse_complement();
     // the forward strand also stays when only the reverse one is used: the
-    // device builds its own reverse complement from it
+    // device builds the reverse complement from it (the host one is made
+    // only on demand, create_reverse_complement)
     if (!has_data && !has_reverse_data) {
         std::string().swap(data_);
         std::string().swap(quality_);
@@ -683,6 +683,22 @@ void Polisher::initialize() {
     for (size_t i = 0; i < sequences_.size(); ++i) sequences_[i]->transmute(has_name[i], has_data[i], has_reverse[i]);
     const double t1 = now_s();
 
+    // the sequence table in device memory: the aligner and the layer
+    // assembly read the reads from there
+    sequence_table_.resize(sequences_.size());
+    for (size_t i = 0; i < sequences_.size(); ++i) {
+        const Sequence& q = *sequences_[i];
+        rb_sequence& e = sequence_table_[i];
+        e.data = q.data().data();
+        e.quality = q.quality().empty() ? nullptr : q.quality().data();
+        e.length = uint32_t(q.data().size());
+        e.forward = has_data[i] ? 1 : 0;
+        e.reverse = has_reverse[i] ? 1 : 0;
+    }
+    if (rb_sequences_stage(ctx_, sequence_table_.data(), sequence_table_.size()) != RB_OK)
+        fail(std::string("[racon::Polisher::initialize] error: ") + rb_last_error(ctx_));
+    staged_ = false;
+    targets_size_ = targets_size;
     find_overlap_breaking_points(overlaps);
     const double t2 = now_s();
 
@@ -720,22 +736,15 @@ void Polisher::initialize() {
         bp_offsets_.push_back(breakpoints_.size());
         o.reset();
     }
-    sequence_table_.resize(sequences_.size());
-    for (size_t i = 0; i < sequences_.size(); ++i) {
-        const Sequence& q = *sequences_[i];
-        rb_sequence& e = sequence_table_[i];
-        e.data = q.data().data();
-        e.quality = q.quality().empty() ? nullptr : q.quality().data();
-        e.length = uint32_t(q.data().size());
-        e.forward = has_data[i] ? 1 : 0;
-        e.reverse = has_reverse[i] ? 1 : 0;
+    // the aligner already staged the layers when every overlap was aligned
+    // on the device; otherwise (SAM CIGARs) they come from these points
+    if (!staged_) {
+        if (rb_poa_stage_overlaps(ctx_, targets_size, layer_overlaps_.data(), layer_overlaps_.size(),
+                                  breakpoints_.data(), bp_offsets_.data(), quality_threshold_, tgs_ ? 1 : 0,
+                                  trim_ ? 1 : 0) != RB_OK)
+            fail(std::string("[racon::Polisher::initialize] error: ") + rb_last_error(ctx_));
+        staged_ = true;
     }
-    if (rb_sequences_stage(ctx_, sequence_table_.data(), sequence_table_.size()) != RB_OK ||
-        rb_poa_stage_overlaps(ctx_, targets_size, layer_overlaps_.data(), layer_overlaps_.size(),
-                              breakpoints_.data(), bp_offsets_.data(), quality_threshold_, tgs_ ? 1 : 0,
-                              trim_ ? 1 : 0) != RB_OK)
-        fail(std::string("[racon::Polisher::initialize] error: ") + rb_last_error(ctx_));
-    staged_ = true;
     const double t3 = now_s();
     stage_s_[0] = t1 - t0;
     stage_s_[1] = t2 - t1;
@@ -749,7 +758,8 @@ void Polisher::assemble_host_layers() {
     for (size_t i = 0; i < targets_size; ++i) first_window[i + 1] += first_window[i];
     for (size_t i = 0; i < layer_overlaps_.size(); ++i) {
         const rb_layer_overlap& o = layer_overlaps_[i];
-        const Sequence& s = *sequences_[o.q_id];
+        Sequence& s = *sequences_[o.q_id];
+        if (o.strand) s.create_reverse_complement();
         std::vector<std::pair<uint32_t, uint32_t>> bp;
         for (uint64_t x = bp_offsets_[i]; x < bp_offsets_[i + 1]; x += 2)
             bp.emplace_back(breakpoints_[x], breakpoints_[x + 1]);
@@ -775,10 +785,13 @@ void Polisher::assemble_host_layers() {
     }
 }
 
-// Device alignment of every overlap without a CIGAR, device CIGAR walk for
-// the others (src/polisher.cpp:462-484 -> src/overlap.cpp:179-203).
+// Device alignment of every overlap without a CIGAR, from the sequence
+// table in device memory; device CIGAR walk for the others
+// (src/polisher.cpp:462-484 -> src/overlap.cpp:179-203). When every overlap
+// is aligned, the breaking points also become window layers on the device
+// in the same call, and only a copy comes back to the host overlaps.
 void Polisher::find_overlap_breaking_points(std::vector<std::unique_ptr<Overlap>>& overlaps) {
-    std::vector<rb_pair> pairs;
+    std::vector<rb_store_pair> pairs;
     std::vector<size_t> pair_of;
     std::vector<rb_cigar_overlap> cig;
     std::vector<size_t> cig_of;
@@ -788,15 +801,14 @@ void Polisher::find_overlap_breaking_points(std::vector<std::unique_ptr<Overlap>
         if (!o.breaking_points.empty()) continue;
         const uint32_t q_offset = o.strand ? o.q_length - o.q_end : o.q_begin;
         if (o.cigar.empty()) {
-            const Sequence& q = *sequences_[o.q_id];
-            const Sequence& t = *sequences_[o.t_id];
-            rb_pair p;
-            p.query = o.strand ? q.reverse_complement().data() + (o.q_length - o.q_end) : q.data().data() + o.q_begin;
-            p.query_length = o.q_end - o.q_begin;
-            p.target = t.data().data() + o.t_begin;
-            p.target_length = o.t_end - o.t_begin;
-            p.q_offset = q_offset;
+            rb_store_pair p;
+            p.q_id = uint32_t(o.q_id);
+            p.q_begin = o.q_begin;
+            p.q_end = o.q_end;
+            p.t_id = uint32_t(o.t_id);
             p.t_begin = o.t_begin;
+            p.t_end = o.t_end;
+            p.strand = o.strand ? 1u : 0u;
             pairs.push_back(p);
             pair_of.push_back(i);
         } else {
@@ -810,18 +822,36 @@ void Polisher::find_overlap_breaking_points(std::vector<std::unique_ptr<Overlap>
             cig_of.push_back(i);
         }
     }
+    if (cig.empty() && pairs.size() == overlaps.size()) {
+        // every overlap aligned here: layers staged on the device as well
+        rb_aln_result r;
+        if (rb_poa_stage_alignments(ctx_, targets_size_, pairs.data(), pairs.size(), quality_threshold_,
+                                    tgs_ ? 1 : 0, trim_ ? 1 : 0, &r) != RB_OK)
+            fail(std::string("[racon::Overlap::find_breaking_points] error: ") + rb_last_error(ctx_));
+        for (size_t k = 0; k < pairs.size(); ++k) {
+            Overlap& o = *overlaps[pair_of[k]];
+            for (uint64_t x = r.bp_offsets[k]; x < r.bp_offsets[k + 1]; x += 2)
+                o.breaking_points.emplace_back(r.breakpoints[x], r.breakpoints[x + 1]);
+        }
+        staged_ = true;
+        for (auto& o : overlaps) std::string().swap(o->cigar);
+        return;
+    }
     // batches bounded by bases so device buffers stay modest
     const uint64_t kBatchBases = uint64_t(1) << 31;
     size_t b = 0;
     while (b < pairs.size()) {
         size_t e = b;
         uint64_t bases = 0;
-        while (e < pairs.size() && (e == b || bases + pairs[e].query_length + pairs[e].target_length <= kBatchBases)) {
-            bases += pairs[e].query_length + pairs[e].target_length;
+        while (e < pairs.size()) {
+            const uint64_t pb = uint64_t(pairs[e].q_end - pairs[e].q_begin) + (pairs[e].t_end - pairs[e].t_begin);
+            if (e > b && bases + pb > kBatchBases) break;
+            bases += pb;
             ++e;
         }
         rb_aln_result r;
-        if (rb_align_batch(ctx_, pairs.data() + b, e - b, 0, &r) != RB_OK)
+        if (rb_align_stage_overlaps(ctx_, pairs.data() + b, e - b, 0) != RB_OK || rb_align_run(ctx_) != RB_OK ||
+            rb_align_fetch(ctx_, &r) != RB_OK)
             fail(std::string("[racon::Overlap::find_breaking_points] error: ") + rb_last_error(ctx_));
         for (size_t k = b; k < e; ++k) {
             Overlap& o = *overlaps[pair_of[k]];

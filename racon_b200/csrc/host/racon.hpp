@@ -139,6 +139,7 @@ protected:
     std::vector<uint32_t> breakpoints_;
     std::vector<uint64_t> bp_offsets_;
     bool staged_ = false;
+    size_t targets_size_ = 0;
 
     uint32_t num_threads_;
     int device_ = 0;

@@ -44,7 +44,7 @@
 namespace rb {
 namespace {
 
-constexpr uint64_t kNone = ~0ull;
+constexpr uint64_t kNone = kNotStaged;
 constexpr uint32_t kDropped = ~0u;
 
 // Errors found by the kernels; the first one is kept with its overlap index.
@@ -57,12 +57,6 @@ enum LayerStatus : uint32_t {
     kLsLongLayer = 5,      // layer longer than 65535 bases
     kLsManyPoints = 6,     // more breaking-point pairs than candidate slots
     kLsBadQuality = 7,     // a quality byte outside '!'..'~' in a kept layer or a backbone
-};
-
-struct SeqDev {
-    uint64_t fwd, fq, rev, rq;  // store offsets, kNone when absent
-    uint32_t len;
-    uint32_t pad;
 };
 
 struct OvlDev {
@@ -436,7 +430,98 @@ void LayerEngine::stage_sequences(const rb_sequence* seqs, size_t n, PoaEngine& 
         fq_[i] = tab[i].fq;
     }
     store_bytes_ = dev_bytes;
+    host_tab_ = std::move(tab);
     nseq_ = n;
+}
+
+SeqStore LayerEngine::store() const {
+    SeqStore st;
+    st.bytes = d_store_.as<uint8_t>();
+    st.seqs = d_seqs_.as<SeqDev>();
+    st.host = host_tab_.data();
+    st.n = nseq_;
+    return st;
+}
+
+void LayerEngine::assemble_aligned(size_t n_targets, const rb_store_pair* pairs, size_t n, uint32_t window_length,
+                                   double quality_threshold, int tgs, int trim, NwEngine& nw, PoaEngine& poa,
+                                   rb_aln_result* out) {
+    poa.forget();
+    if (n > 0 && !pairs) throw Error{RB_ERR_ARG, "rb_poa_stage_alignments: pairs is NULL"};
+    if (n_targets > nseq_) throw Error{RB_ERR_ARG, "rb_poa_stage_alignments: more targets than staged sequences"};
+    if (window_length == 0) throw Error{RB_ERR_ARG, "rb_poa_stage_alignments: window length is 0"};
+    // candidate slots in overlap order: one per window the target span
+    // touches (the aligner's breaking-point slots)
+    std::vector<uint64_t> cand(n + 1, 0);
+    for (size_t i = 0; i < n; ++i) {
+        const uint32_t tb = pairs[i].t_begin, te = pairs[i].t_end;
+        const uint64_t segs = te > tb ? (uint64_t(te) - 1) / window_length - tb / window_length + 1 : 0;
+        cand[i + 1] = cand[i] + segs;
+    }
+    if (cand[n] >= kDropped) throw Error{RB_ERR_ARG, "rb_poa_stage_alignments: more than 2^32 - 1 layer candidates"};
+    begin(n_targets, window_length, quality_threshold, cand[n]);
+    if (out) {
+        out_dist_.clear();
+        out_bp_.clear();
+        out_bp_off_.assign(1, 0);
+    }
+    const SeqStore st = store();
+    // batches bounded by bases so the aligner's buffers stay modest
+    const uint64_t kBatchBases = uint64_t(1) << 31;
+    std::vector<OvlDev> od;
+    size_t b = 0;
+    while (b < n) {
+        size_t e = b;
+        uint64_t bases = 0;
+        while (e < n) {
+            const uint64_t pb = uint64_t(pairs[e].q_end - pairs[e].q_begin) + (pairs[e].t_end - pairs[e].t_begin);
+            if (e > b && bases + pb > kBatchBases) break;
+            bases += pb;
+            ++e;
+        }
+        nw.stage_store(pairs + b, e - b, 0, window_length, st);
+        nw.run();
+        const NwPairDev* pd = nw.pairs();
+        od.resize(e - b);
+        for (size_t k = 0; k < e - b; ++k) {
+            const rb_store_pair& p = pairs[b + k];
+            OvlDev& d = od[k];
+            d.bp_off = pd[k].bp_off;
+            d.cand = cand[b + k];
+            d.q_id = p.q_id;
+            d.t_id = p.t_id;
+            d.strand = p.strand ? 1u : 0u;
+            d.cnt = 0;
+            d.cnt_idx = uint32_t(k);
+            d.cap = uint32_t(cand[b + k + 1] - cand[b + k]);
+        }
+        h_bp_.reserve(od.size() * sizeof(OvlDev));
+        memcpy(h_bp_.ptr, od.data(), od.size() * sizeof(OvlDev));
+        d_ovl_.reserve(od.size() * sizeof(OvlDev));
+        check_cuda(cudaMemcpyAsync(d_ovl_.ptr, h_bp_.ptr, od.size() * sizeof(OvlDev), cudaMemcpyHostToDevice,
+                                   stream_),
+                   "H2D overlaps");
+        stats_.h2d_bytes += od.size() * sizeof(OvlDev);
+        add_candidates(nw.bp_slots(), nw.bp_counts(), d_ovl_.ptr, e - b);
+        if (out) {
+            rb_aln_result r;
+            nw.fetch(&r);
+            for (size_t k = 0; k < e - b; ++k) {
+                out_dist_.push_back(r.edit_distance[k]);
+                out_bp_.insert(out_bp_.end(), r.breakpoints + r.bp_offsets[k], r.breakpoints + r.bp_offsets[k + 1]);
+                out_bp_off_.push_back(out_bp_.size());
+            }
+        }
+        b = e;
+    }
+    finish(tgs, trim, poa);
+    if (out) {
+        out->edit_distance = out_dist_.data();
+        out->breakpoints = out_bp_.data();
+        out->bp_offsets = out_bp_off_.data();
+        out->cigars = nullptr;
+        out->cigar_offsets = nullptr;
+    }
 }
 
 void LayerEngine::assemble(size_t n_targets, const rb_layer_overlap* ovl, size_t n, const uint32_t* bps,

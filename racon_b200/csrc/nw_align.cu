@@ -902,6 +902,64 @@ __global__ void __launch_bounds__(32) nw_distance_noalloc_kernel(const char* q, 
     if (lane == 0) *out = d;
 }
 
+// Store offsets of one pair's query and target spans (rb_align_stage_overlaps).
+struct NwStoreSrc {
+    uint64_t q_src, t_src;
+};
+
+// Symbol codes of pairs cut from the staged sequence table: bytes are
+// numbered by first appearance in the query, then the target (the numbering
+// NwEngine::stage gives on the host), one warp per pair. First appearances
+// come from one pass over 32-byte chunks in order: the lowest lane holding a
+// byte value not seen before records its position. A pair with more than
+// kMaxSym distinct bytes sets status[0] = 1 and is not encoded.
+__global__ void __launch_bounds__(256) nw_encode_kernel(const uint8_t* store, const NwStoreSrc* src,
+                                                        NwPairDev* pairs, uint8_t* codes, uint32_t n,
+                                                        unsigned int* status) {
+    __shared__ uint32_t first_pos[8][256];
+    __shared__ uint8_t code[8][256];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* fp = first_pos[wib];
+    uint8_t* cd = code[wib];
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+        const NwStoreSrc sp = src[i];
+        const uint32_t m = pairs[i].m, nt = pairs[i].n;
+        const uint64_t q_off = pairs[i].q_off, t_off = pairs[i].t_off;
+        for (int v = lane; v < 256; v += 32) fp[v] = 0xFFFFFFFFu;
+        __syncwarp();
+        const uint32_t total = m + nt;
+        for (uint32_t k0 = 0; k0 < total; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            uint32_t c = 0x100u + uint32_t(lane);  // matches no byte value
+            if (k < total) c = k < m ? store[sp.q_src + k] : store[sp.t_src + (k - m)];
+            const unsigned same = __match_any_sync(0xffffffffu, c);
+            if (c < 0x100u && __ffs(same) - 1 == lane && fp[c] == 0xFFFFFFFFu) fp[c] = k;
+            __syncwarp();
+        }
+        int present = 0;
+        for (int v = lane; v < 256; v += 32) {
+            const uint32_t p = fp[v];
+            if (p == 0xFFFFFFFFu) continue;
+            int r = 0;
+            for (int u = 0; u < 256; ++u) r += fp[u] < p ? 1 : 0;
+            cd[v] = uint8_t(r);
+            ++present;
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) present += __shfl_xor_sync(0xffffffffu, present, d);
+        __syncwarp();
+        if (present > kMaxSym) {
+            if (lane == 0) status[0] = 1u;
+            continue;
+        }
+        for (uint32_t k = lane; k < m; k += 32) codes[q_off + k] = cd[store[sp.q_src + k]];
+        for (uint32_t k = lane; k < nt; k += 32) codes[t_off + k] = cd[store[sp.t_src + k]];
+        if (lane == 0) pairs[i].nsym = uint32_t(max(present, 1));
+        __syncwarp();
+    }
+}
+
 }  // namespace
 
 NwEngine::NwEngine(const DeviceInfo& dev, cudaStream_t stream) : dev_(dev), stream_(stream) {
@@ -1020,6 +1078,97 @@ void NwEngine::stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t wi
     cudaEventElapsedTime(&ms, ev0_, ev1_);
     stats_.h2d_ms = ms;
     stats_.h2d_bytes = bytes + n * (sizeof(NwPairDev) + sizeof(uint32_t));
+}
+
+void NwEngine::stage_store(const rb_store_pair* pairs, size_t n, int want_cigar, uint32_t window_length,
+                           const SeqStore& st) {
+    if (n > 0 && !pairs) throw Error{RB_ERR_ARG, "rb_align: pairs is NULL"};
+    if (window_length == 0) throw Error{RB_ERR_ARG, "rb_align: window length is 0"};
+    npairs_ = 0;
+    want_cigar_ = want_cigar;
+    window_length_ = window_length;
+    uint64_t bytes = 0, mq_len = 0, bp_slots = 0;
+    max_m_ = max_n_ = 0;
+    h_pairs_.reserve(std::max<size_t>(n, 1) * sizeof(NwPairDev));
+    h_order_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
+    h_src_.reserve(std::max<size_t>(n, 1) * sizeof(NwStoreSrc));
+    NwPairDev* pd = h_pairs_.as<NwPairDev>();
+    NwStoreSrc* src = h_src_.as<NwStoreSrc>();
+    for (size_t i = 0; i < n; ++i) {
+        const rb_store_pair& p = pairs[i];
+        if (p.q_id >= st.n || p.t_id >= st.n) throw Error{RB_ERR_ARG, "rb_align: sequence id out of range"};
+        const SeqDev& q = st.host[p.q_id];
+        const SeqDev& t = st.host[p.t_id];
+        if (p.q_begin > p.q_end || p.q_end > q.len || p.t_begin > p.t_end || p.t_end > t.len)
+            throw Error{RB_ERR_ARG, "rb_align: span outside its sequence"};
+        const uint64_t qbase = p.strand ? q.rev : q.fwd;
+        if (qbase == kNotStaged || t.fwd == kNotStaged)
+            throw Error{RB_ERR_ARG, "rb_align: sequence strand not staged"};
+        const uint32_t m = p.q_end - p.q_begin, tn = p.t_end - p.t_begin;
+        if (m > (1u << 24) || tn > (1u << 24)) throw Error{RB_ERR_ARG, "rb_align: span longer than 2^24 bases"};
+        // query = read span, reverse-complemented for '-' (src/overlap.cpp:193-197)
+        const uint32_t q_offset = p.strand ? q.len - p.q_end : p.q_begin;
+        src[i].q_src = qbase + q_offset;
+        src[i].t_src = t.fwd + p.t_begin;
+        NwPairDev& d = pd[i];
+        d.q_off = bytes;
+        bytes += (m + 15) & ~15u;
+        d.t_off = bytes;
+        bytes += (tn + 15) & ~15u;
+        d.nsym = 1;
+        d.m = m;
+        d.n = tn;
+        d.mq_off = mq_len;
+        mq_len += tn;
+        d.bp_off = bp_slots;
+        if (tn > 0) bp_slots += 4 * ((uint64_t(p.t_begin) + tn - 1) / window_length - p.t_begin / window_length + 1);
+        d.q_offset = q_offset;
+        d.t_begin = p.t_begin;
+        max_m_ = std::max(max_m_, m);
+        max_n_ = std::max(max_n_, tn);
+    }
+    code_bytes_ = bytes;
+    mq_len_ = mq_len;
+    bp_slots_ = bp_slots;
+    uint32_t* order = h_order_.as<uint32_t>();
+    std::iota(order, order + n, 0u);
+    std::sort(order, order + n, [&](uint32_t x, uint32_t y) {
+        const uint64_t wx = uint64_t(pd[x].m + 64) * pd[x].n, wy = uint64_t(pd[y].m + 64) * pd[y].n;
+        return wx != wy ? wx > wy : x < y;
+    });
+    d_codes_.reserve(std::max<uint64_t>(bytes, 16));
+    d_pairs_.reserve(std::max<size_t>(n, 1) * sizeof(NwPairDev));
+    d_src_.reserve(std::max<size_t>(n, 1) * sizeof(NwStoreSrc));
+    d_order_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
+    d_dist_.reserve(std::max<size_t>(n, 1) * sizeof(int32_t));
+    d_mq_.reserve(std::max<uint64_t>(mq_len, 1) * sizeof(int32_t));
+    d_bp_.reserve(std::max<uint64_t>(bp_slots, 1) * sizeof(uint32_t));
+    d_bpcnt_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
+    d_misc_.reserve(64);
+    check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    if (n) {
+        check_cuda(cudaMemcpyAsync(d_pairs_.ptr, pd, n * sizeof(NwPairDev), cudaMemcpyHostToDevice, stream_),
+                   "H2D pairs");
+        check_cuda(cudaMemcpyAsync(d_src_.ptr, src, n * sizeof(NwStoreSrc), cudaMemcpyHostToDevice, stream_),
+                   "H2D pair sources");
+        check_cuda(cudaMemcpyAsync(d_order_.ptr, order, n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_),
+                   "H2D order");
+        check_cuda(cudaMemsetAsync(d_misc_.ptr, 0, 64, stream_), "memset status");
+        const int grid = int(std::max<size_t>(1, std::min<size_t>((n + 7) / 8, size_t(dev_.sm_count) * 8)));
+        nw_encode_kernel<<<grid, 256, 0, stream_>>>(st.bytes, d_src_.as<NwStoreSrc>(), d_pairs_.as<NwPairDev>(),
+                                                    d_codes_.as<uint8_t>(), uint32_t(n), d_misc_.as<unsigned int>());
+        check_cuda(cudaGetLastError(), "nw_encode_kernel");
+    }
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    unsigned int status = 0;
+    if (n) check_cuda(cudaMemcpyAsync(&status, d_misc_.ptr, 4, cudaMemcpyDeviceToHost, stream_), "D2H status");
+    check_cuda(cudaStreamSynchronize(stream_), "stage sync");
+    if (status) throw Error{RB_ERR_ARG, "rb_align: more than 32 distinct symbols in a pair"};
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.h2d_ms = ms;
+    stats_.h2d_bytes = n * (sizeof(NwPairDev) + sizeof(NwStoreSrc) + sizeof(uint32_t));
+    npairs_ = n;
 }
 
 void NwEngine::reserve_scratch(uint32_t max_m, uint32_t max_n) {

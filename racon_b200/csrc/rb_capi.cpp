@@ -209,6 +209,18 @@ int rb_poa_batch(rb_ctx* ctx, const rb_window* windows, size_t n, int trim, rb_p
 int rb_sequences_stage(rb_ctx* ctx, const rb_sequence* sequences, size_t n) {
     return guarded(ctx, [&]() { ctx->layers->stage_sequences(sequences, n, *ctx->poa); });
 }
+int rb_align_stage_overlaps(rb_ctx* ctx, const rb_store_pair* pairs, size_t n, int want_cigar) {
+    return guarded(ctx, [&]() {
+        ctx->nw->stage_store(pairs, n, want_cigar, ctx->params.window_length, ctx->layers->store());
+    });
+}
+int rb_poa_stage_alignments(rb_ctx* ctx, size_t n_targets, const rb_store_pair* pairs, size_t n,
+                            double quality_threshold, int tgs, int trim, rb_aln_result* breakpoints) {
+    return guarded(ctx, [&]() {
+        ctx->layers->assemble_aligned(n_targets, pairs, n, ctx->params.window_length, quality_threshold, tgs, trim,
+                                      *ctx->nw, *ctx->poa, breakpoints);
+    });
+}
 int rb_poa_stage_overlaps(rb_ctx* ctx, size_t n_targets, const rb_layer_overlap* overlaps, size_t n,
                           const uint32_t* breakpoints, const uint64_t* bp_offsets, double quality_threshold,
                           int tgs, int trim) {

@@ -47,6 +47,25 @@ struct DeviceInfo {
     size_t smem_optin = 0;
 };
 
+// ----- device sequence store (layers.cu) -----
+// One entry of the staged sequence table: offsets of the forward bases and
+// quality and of the reverse complement and reversed quality in the store.
+constexpr uint64_t kNotStaged = ~0ull;
+
+struct SeqDev {
+    uint64_t fwd, fq, rev, rq;  // store offsets, kNotStaged when absent
+    uint32_t len;
+    uint32_t pad;
+};
+
+// The staged table as the aligner and the layer assembly read it.
+struct SeqStore {
+    const uint8_t* bytes = nullptr;   // device
+    const SeqDev* seqs = nullptr;     // device
+    const SeqDev* host = nullptr;     // host copy of seqs
+    size_t n = 0;
+};
+
 // ----- overlap alignment engine (nw_align.cu) -----
 struct NwPairDev {
     uint64_t q_off, t_off;  // offsets of the encoded query / target in the code buffer
@@ -62,8 +81,16 @@ public:
     explicit NwEngine(const DeviceInfo& dev, cudaStream_t stream);
     ~NwEngine();
     void stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t window_length);
+    // Pairs cut from the staged sequence table and encoded on the device.
+    void stage_store(const rb_store_pair* pairs, size_t n, int want_cigar, uint32_t window_length,
+                     const SeqStore& st);
     void run();
     void fetch(rb_aln_result* out);
+    // Breaking points of the last run on the device: pair i's (t, q) values
+    // at bp_slots()[pairs()[i].bp_off ...], bp_counts()[i] of them.
+    const uint32_t* bp_slots() const { return d_bp_.as<uint32_t>(); }
+    const uint32_t* bp_counts() const { return d_bpcnt_.as<uint32_t>(); }
+    const NwPairDev* pairs() const { return h_pairs_.as<NwPairDev>(); }
     // breaking points straight from SAM CIGARs (no alignment)
     void cigar_breakpoints(const rb_cigar_overlap* ovl, size_t n, uint32_t window_length,
                            rb_aln_result* out);
@@ -79,9 +106,9 @@ private:
     uint32_t window_length_ = 500;
     uint32_t max_m_ = 0, max_n_ = 0;
     uint64_t code_bytes_ = 0, mq_len_ = 0, bp_slots_ = 0;
-    HostBuf h_codes_, h_pairs_, h_order_;
+    HostBuf h_codes_, h_pairs_, h_order_, h_src_;
     HostBuf h_dist_, h_bp_, h_bpcnt_, h_cig_, h_cigoff_, h_misc_;
-    DevBuf d_codes_, d_pairs_, d_order_, d_dist_, d_mq_, d_bp_, d_bpcnt_;
+    DevBuf d_codes_, d_pairs_, d_src_, d_order_, d_dist_, d_mq_, d_bp_, d_bpcnt_;
     DevBuf d_tasks_[2], d_misc_, d_scratch_, d_ciglen_, d_cigoff_, d_cig_;
     size_t scratch_warps_ = 0, scratch_stride_ = 0;
     std::vector<int32_t> dist_;
@@ -164,6 +191,7 @@ private:
 };
 
 // ----- device layer assembly (layers.cu) -----
+
 class LayerEngine {
 public:
     LayerEngine(const DeviceInfo& dev, cudaStream_t stream);
@@ -176,6 +204,14 @@ public:
     void assemble(size_t n_targets, const rb_layer_overlap* ovl, size_t n, const uint32_t* bps,
                   const uint64_t* bp_offsets, uint32_t window_length, double quality_threshold, int tgs, int trim,
                   PoaEngine& poa);
+    // The same from alignments of pairs cut from the store: each batch's
+    // breaking points go from the aligner's device buffers straight to the
+    // layer candidates. out (may be NULL) receives edit distances and
+    // breaking points on the host.
+    void assemble_aligned(size_t n_targets, const rb_store_pair* pairs, size_t n, uint32_t window_length,
+                          double quality_threshold, int tgs, int trim, NwEngine& nw, PoaEngine& poa,
+                          rb_aln_result* out);
+    SeqStore store() const;
     const rb_stats& stats() const { return stats_; }
     const rb_stats& sequence_stats() const { return seq_stats_; }
 
@@ -200,6 +236,10 @@ private:
     float cand_ms_ = 0;
     std::vector<uint32_t> lens_;
     std::vector<uint64_t> fwd_, fq_, first_window_;
+    std::vector<SeqDev> host_tab_;
+    std::vector<int32_t> out_dist_;
+    std::vector<uint32_t> out_bp_;
+    std::vector<uint64_t> out_bp_off_;
     HostBuf h_store_, h_misc_, h_bp_, h_fw_, h_lay_, h_perm_;
     DevBuf d_store_, d_seqs_, d_list_, d_bp_, d_ovl_, d_fw_, d_cand_, d_cand_win_, d_win_, d_lay_, d_final_;
     rb_stats stats_{}, seq_stats_{};
