@@ -496,6 +496,7 @@ def main():
     job = racon_b200.Job(*paths, fragment=args.config == 3, window_length=w, match=m, mismatch=x, gap=g,
                          device=local)
     n_win, n_layers, layer_bases, bb_bases = job.layer_stats()
+    jst = job.device_stats()
     ctx = racon_b200.Context(local, m, x, g, w)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
@@ -635,7 +636,12 @@ def main():
                     "frac": achieved_tops / int_peak_tops, "gcups": gcups,
                     "note": "peak = SMs x 128 int32 lanes x median SM clock under load; ~6 int ops per cell"},
         "clocks": clk,
-        "stages_s": {"load": job.stage_seconds[0], "align": job.stage_seconds[1], "layers": job.stage_seconds[2]},
+        "stages_s": {"load": job.stage_seconds[0], "align": job.stage_seconds[1], "layers": job.stage_seconds[2],
+                     "note": "align = sequence table to the device, overlap alignment and (PAF/MHAP) the "
+                             "device layer assembly; layers = the host's window records"},
+        "job_device_ms": {"align_kernels": jst["align"].kernel_ms, "align_h2d": jst["align"].h2d_ms,
+                          "align_d2h": jst["align"].d2h_ms, "align_launches": jst["align"].launches,
+                          "sequences_h2d": jst["sequences"].h2d_ms, "layer_kernels": jst["layers"].kernel_ms},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = [job.window(i) for i in range(min(args.cpu_sample, n_win))]

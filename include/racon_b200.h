@@ -311,6 +311,10 @@ size_t rb_job_windows(const rb_job* job, const rb_window** windows);
 int rb_job_layer_input(const rb_job* job, const rb_sequence** sequences, size_t* n_sequences, size_t* n_targets,
                        const rb_layer_overlap** overlaps, size_t* n_overlaps, const uint32_t** breakpoints,
                        const uint64_t** bp_offsets, int* tgs);
+/* The device context a job was prepared on (borrowed; valid until
+ * rb_job_free): its rb_align_stats / rb_layer_stats / rb_sequence_stats
+ * describe the job's own alignment and layer assembly. */
+rb_ctx* rb_job_context(const rb_job* job);
 void rb_job_free(rb_job* job);
 void rb_free(void* p);
 

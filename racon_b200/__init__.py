@@ -176,6 +176,8 @@ def load():
     lib.rb_job_windows.restype = ctypes.c_size_t
     lib.rb_job_windows.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(_Window))]
     lib.rb_job_free.argtypes = [vp]
+    lib.rb_job_context.restype = vp
+    lib.rb_job_context.argtypes = [vp]
     lib.rb_free.argtypes = [vp]
     lib.rb_server_create.restype = vp
     lib.rb_server_create.argtypes = [ctypes.POINTER(_ServerParams)]
@@ -519,6 +521,19 @@ class Job:
             ends.append(w.ends[j])
         return {"backbone": bb, "backbone_quality": bq, "layers": layers, "qualities": quals, "begins": begins,
                 "ends": ends, "tgs": w.tgs, "id": w.id, "rank": w.rank}
+
+    def device_stats(self):
+        """Counters of the job's own device work: {"align", "layers",
+        "sequences"} -> Stats (rb_align_stats, rb_layer_stats and
+        rb_sequence_stats of the job's context; align covers the last batch)."""
+        ctx = self.lib.rb_job_context(self.ptr)
+        out = {}
+        for name, fn in (("align", self.lib.rb_align_stats), ("layers", self.lib.rb_layer_stats),
+                         ("sequences", self.lib.rb_sequence_stats)):
+            s = Stats()
+            fn(ctypes.c_void_p(ctx), ctypes.byref(s))
+            out[name] = s
+        return out
 
     def layer_input(self):
         """The job as device layer assembly input (rb_job_layer_input): ctypes

@@ -1096,4 +1096,6 @@ extern "C" int rb_job_layer_input(const rb_job* job, const rb_sequence** sequenc
     return RB_OK;
 }
 
+extern "C" rb_ctx* rb_job_context(const rb_job* job) { return job ? job->polisher->ctx_ : nullptr; }
+
 extern "C" void rb_job_free(rb_job* job) { delete job; }

@@ -91,6 +91,7 @@ public:
         uint32_t num_threads, uint32_t cuda_batches, bool cuda_banded_alignment,
         uint32_t cudaaligner_batches, uint32_t cudaaligner_band_width);
     friend struct ::rb_job;
+    friend rb_ctx* ::rb_job_context(const rb_job*);
     friend int ::rb_job_layer_input(const rb_job*, const rb_sequence**, size_t*, size_t*,
                                     const rb_layer_overlap**, size_t*, const uint32_t**, const uint64_t**, int*);
     friend std::unique_ptr<Polisher> createPolisherOnContext(rb_ctx* ctx, int device,
