@@ -204,11 +204,24 @@ struct SweepIO {
     int bw;            // leaf: blocks stored per column
 };
 
+// Where a kDistance sweep gave up: the bottom row of the strip whose cells
+// all exceeded k, and their minimum (row = -1: it did not give up early).
+struct SweepFail {
+    int row = -1;
+    int min = 0;
+};
+
 // Banded block sweep of one subproblem by one warp. MODE kDistance returns
-// the value of cell (m-1, n-1) (INT_MAX if the band never reached it).
+// the value of cell (m-1, n-1) (INT_MAX if the band never reached it). It
+// also stops early, returning INT_MAX, once every computed cell of a full
+// strip's bottom row R exceeds k and so does the left boundary (R + 1): costs
+// never fall along a path, every path of cost <= k stays inside the band, and
+// a computed in-band value is at most the cost of any path to it inside the
+// band, so no path of cost <= k crosses row R. (Out-of-band cells only lower
+// the minimum.) The distance of a pass that reaches the end is unchanged.
 template <int MODE>
 __device__ int warp_sweep(const SweepIO& io, const Band& B, const WarpScratch& ws, int lane,
-                          unsigned int* counters) {
+                          unsigned int* counters, SweepFail* fail = nullptr) {
     int result = INT_MAX;
     const int nstrips = (B.nb + 31) / 32;
     const int m = B.m, n = B.n;
@@ -242,6 +255,7 @@ __device__ int warp_sweep(const SweepIO& io, const Band& B, const WarpScratch& w
 
         u64 pv = 0, mv = 0;
         int score = 0;
+        int bottom_min = INT_MAX;  // kDistance, lane 31: minimum of the strip's bottom row
         bool started = false;
         int in_pack = 0;  // previous step of lane-1: (score << 3) | (processed << 2) | (hout + 1)
         const int steps = (s_hi - s_lo) + 32;
@@ -293,6 +307,7 @@ __device__ int warp_sweep(const SweepIO& io, const Band& B, const WarpScratch& w
                 if (MODE == kDistance && b == B.nb - 1 && c == n - 1) {
                     result = block_value(pv, mv, score, (m - 1) & 63);
                 }
+                if (MODE == kDistance && lane == 31) bottom_min = min(bottom_min, score);
                 if (lane == 31) {
                     carry_h_out[c] = int8_t(hout);
                     carry_s_out[c] = score;
@@ -302,12 +317,38 @@ __device__ int warp_sweep(const SweepIO& io, const Band& B, const WarpScratch& w
             in_pack = __shfl_up_sync(kFull, pack, 1);
         }
         __syncwarp();
+        if (MODE == kDistance && 32 * s + 31 < B.nb - 1) {
+            const int row_min = __shfl_sync(kFull, bottom_min, 31);
+            const int R = 64 * (32 * s + 31) + 63;
+            if (row_min > B.k && R + 1 > B.k) {
+                if (fail) {
+                    fail->row = R;
+                    fail->min = row_min;
+                }
+                result = INT_MAX;
+                break;
+            }
+        }
     }
     if (MODE == kDistance) {
         for (int o = 16; o > 0; o >>= 1) result = min(result, __shfl_xor_sync(kFull, result, o));
     }
     (void)counters;
     return result;
+}
+
+// k of the next distance pass after a pass with k failed: at least twice k;
+// when the pass gave up at row f.row with minimum cost f.min, the cost per
+// row so far projected over the longer side (x 1.1), up to 8k. Any k gives
+// the same distance once k >= distance; this only picks how many passes.
+__device__ __forceinline__ int next_k(int k, const SweepFail& f, int m, int n) {
+    long long nk = 2LL * k;
+    if (f.row >= 0) {
+        const double est = double(f.min) * double(max(m, n)) / double(f.row + 1);
+        const long long want = ((long long)(est * 1.1) + 63) / 64 * 64;
+        nk = max(nk, min(8LL * k, want));
+    }
+    return int(min(nk, 1LL << 30));
 }
 
 __device__ void fill_deleted(int32_t* mq, int from, int count, int lane) {
@@ -563,9 +604,10 @@ nw_distance_kernel(NwDevArgs a) {
         int d = INT_MAX;
         while (true) {
             const Band B = make_band(m, n, k);
-            d = warp_sweep<kDistance>(io, B, ws, lane, a.counters);
+            SweepFail f;
+            d = warp_sweep<kDistance>(io, B, ws, lane, a.counters, &f);
             if (d <= k) break;
-            k *= 2;
+            k = next_k(k, f, m, n);
         }
         if (lane == 0) a.dist[pi] = d;
     }
@@ -895,9 +937,10 @@ __global__ void __launch_bounds__(32) nw_distance_noalloc_kernel(const char* q, 
     int d;
     while (true) {
         const Band B = make_band(int(m), int(n), k);
-        d = warp_sweep<kDistance>(io, B, ws, lane, nullptr);
+        SweepFail f;
+        d = warp_sweep<kDistance>(io, B, ws, lane, nullptr, &f);
         if (d <= k) break;
-        k *= 2;
+        k = next_k(k, f, int(m), int(n));
     }
     if (lane == 0) *out = d;
 }
