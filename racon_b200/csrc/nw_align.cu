@@ -651,47 +651,67 @@ nw_level_kernel(NwDevArgs a) {
 
 // Breaking points from mq: one window segment per floor(t / w); for each
 // segment with a match, (first match t, q) and (last match t + 1, q + 1).
-__global__ void nw_breakpoints_kernel(NwDevArgs a) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.npairs) return;
-    const NwPairDev P = a.pairs[i];
-    uint32_t* out = a.bp + P.bp_off;
-    uint32_t cnt = 0;
-    if (P.m != 0 && P.n != 0) {
-        const int32_t* mq = a.mq + P.mq_off;
-        const uint32_t w = a.window_length;
-        int64_t cur = -1;
-        uint32_t ft = 0, fq = 0, lt = 0, lq = 0;
-        for (uint32_t c = 0; c < P.n; ++c) {
-            const int32_t v = mq[c];
-            if (v < 0) continue;
-            const uint32_t t = P.t_begin + c;
-            const int64_t sgm = t / w;
-            if (sgm != cur) {
-                if (cur >= 0) {
-                    out[cnt++] = ft;
-                    out[cnt++] = fq;
-                    out[cnt++] = lt;
-                    out[cnt++] = lq;
+// Window breaking points of each pair from its match table, one warp per
+// pair over 32-position chunks: racon's walk (src/overlap.cpp:244-290) emits,
+// per window the target touches, the first matched (t, q) and the last
+// matched (t + 1, q + 1). A matched position opens a window segment when the
+// previous matched position (the highest matched lane below, or the carry of
+// earlier chunks) lies in another window; it writes its segment's first pair
+// and closes the previous segment's last pair.
+__global__ void __launch_bounds__(256) nw_breakpoints_kernel(NwDevArgs a) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below_mask = (1u << lane) - 1u;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.npairs; i += nwarps) {
+        const NwPairDev P = a.pairs[i];
+        uint32_t* out = a.bp + P.bp_off;
+        uint32_t segs = 0;
+        if (P.m != 0 && P.n != 0) {
+            const int32_t* mq = a.mq + P.mq_off;
+            const uint32_t w = a.window_length;
+            uint32_t carry_sgm = 0xFFFFFFFFu, carry_t = 0, carry_q = 0;
+            for (uint32_t c0 = 0; c0 < P.n; c0 += 32) {
+                const uint32_t c = c0 + lane;
+                const int32_t v = c < P.n ? mq[c] : -1;
+                const bool matched = v >= 0;
+                const uint32_t t = P.t_begin + c;
+                const uint32_t q = P.q_offset + uint32_t(v);
+                const uint32_t sgm = t / w;
+                const unsigned mm = __ballot_sync(kFull, matched);
+                const unsigned below = mm & below_mask;
+                const int p = below ? 31 - __clz(below) : 0;
+                const uint32_t p_sgm = __shfl_sync(kFull, sgm, p);
+                const uint32_t p_t = __shfl_sync(kFull, t, p);
+                const uint32_t p_q = __shfl_sync(kFull, q, p);
+                const uint32_t prev_sgm = below ? p_sgm : carry_sgm;
+                const bool first = matched && sgm != prev_sgm;
+                const unsigned fm = __ballot_sync(kFull, first);
+                if (first) {
+                    const uint32_t idx = segs + __popc(fm & below_mask);
+                    out[4 * idx] = t;
+                    out[4 * idx + 1] = q;
+                    if (idx > 0) {
+                        out[4 * (idx - 1) + 2] = (below ? p_t : carry_t) + 1;
+                        out[4 * (idx - 1) + 3] = (below ? p_q : carry_q) + 1;
+                    }
                 }
-                cur = sgm;
-                ft = t;
-                fq = P.q_offset + uint32_t(v);
+                segs += __popc(fm);
+                if (mm) {
+                    const int hl = 31 - __clz(mm);
+                    carry_sgm = __shfl_sync(kFull, sgm, hl);
+                    carry_t = __shfl_sync(kFull, t, hl);
+                    carry_q = __shfl_sync(kFull, q, hl);
+                }
             }
-            lt = t + 1;
-            lq = P.q_offset + uint32_t(v) + 1;
+            if (segs > 0 && lane == 0) {
+                out[4 * (segs - 1) + 2] = carry_t + 1;
+                out[4 * (segs - 1) + 3] = carry_q + 1;
+            }
         }
-        if (cur >= 0) {
-            out[cnt++] = ft;
-            out[cnt++] = fq;
-            out[cnt++] = lt;
-            out[cnt++] = lq;
-        }
+        if (lane == 0) a.bp_count[i] = 4 * segs;
     }
-    a.bp_count[i] = cnt;
 }
 
-// CIGAR from mq (standard M/I/D). pass 0 counts characters, pass 1 writes.
 __device__ int put_run(char* dst, int pos, bool write, int len, char op) {
     char tmp[12];
     int d = 0;
@@ -706,45 +726,104 @@ __device__ int put_run(char* dst, int pos, bool write, int len, char op) {
     return pos + 1;
 }
 
-__global__ void nw_cigar_kernel(NwDevArgs a, uint64_t* lens, const uint64_t* offs, char* out,
-                                int write) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.npairs) return;
-    const NwPairDev P = a.pairs[i];
-    if (P.m == 0 || P.n == 0) {
-        if (!write) lens[i] = 0;
-        return;
+__device__ __forceinline__ int decimal_digits(uint32_t x) {
+    int d = 1;
+    while (x >= 10) {
+        x /= 10;
+        ++d;
     }
-    const int32_t* mq = a.mq + P.mq_off;
-    char* dst = write ? out + offs[i] : nullptr;
-    int pos = 0;
-    char run_op = 0;
-    int run_len = 0;
-    auto emit = [&](char op, int len) {
-        if (op == run_op) {
-            run_len += len;
-        } else {
-            if (run_len > 0) pos = put_run(dst, pos, write != 0, run_len, run_op);
-            run_op = op;
-            run_len = len;
+    return d;
+}
+
+// Standard CIGAR (M/I/D runs) of each pair from its match table, one warp
+// per pair over 32-position chunks; write = 0 counts the characters into
+// lens, write = 1 writes them at offs. The sequential walk it restates: per
+// target position an insertion run before a matched position (the query
+// positions skipped since the previous match), then M, or D when unmatched;
+// equal neighbouring ops merge, and trailing query positions end with I.
+// An M/D run therefore starts where the op changes or an insertion comes
+// first; each such position closes the previous run and emits its own I run,
+// and a warp prefix sum of their text lengths gives every lane's offset.
+__global__ void __launch_bounds__(256) nw_cigar_kernel(NwDevArgs a, uint64_t* lens, const uint64_t* offs, char* out,
+                                                       int write) {
+    const int lane = threadIdx.x & 31;
+    const unsigned below_mask = (1u << lane) - 1u;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.npairs; i += nwarps) {
+        const NwPairDev P = a.pairs[i];
+        if (P.m == 0 || P.n == 0) {
+            if (!write && lane == 0) lens[i] = 0;
+            continue;
         }
-    };
-    int qprev = -1;
-    for (uint32_t c = 0; c < P.n; ++c) {
-        const int v = mq[c];
-        if (v >= 0) {
-            const int ins = v - qprev - 1;
-            if (ins > 0) emit('I', ins);
-            emit('M', 1);
-            qprev = v;
-        } else {
-            emit('D', 1);
+        const int32_t* mq = a.mq + P.mq_off;
+        char* dst = write ? out + offs[i] : nullptr;
+        const uint32_t n = P.n;
+        uint64_t pos = 0;           // characters before this chunk
+        int carry_v = -1;           // last matched query position so far
+        int carry_op = -1;          // op of the position before the chunk (0 = M, 1 = D)
+        uint32_t run_start = 0;     // first position of the open M/D run
+        int run_op = -1;            // its op (-1: none yet)
+        for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+            const uint32_t c = c0 + lane;
+            const bool valid = c < n;
+            const int v = valid ? mq[c] : -1;
+            const bool matched = v >= 0;
+            const int op = matched ? 0 : 1;
+            const unsigned mm = __ballot_sync(kFull, matched);
+            const unsigned mbelow = mm & below_mask;
+            const int p_v = __shfl_sync(kFull, v, mbelow ? 31 - __clz(mbelow) : 0);
+            const int prev_v = mbelow ? p_v : carry_v;
+            const int ins = matched ? v - prev_v - 1 : 0;
+            const int up_op = __shfl_up_sync(kFull, op, 1);
+            const int prev_op = lane > 0 ? up_op : carry_op;
+            const bool start = valid && (c == 0 || op != prev_op || ins > 0);
+            const unsigned sm = __ballot_sync(kFull, start);
+            const unsigned sbelow = sm & below_mask;
+            const int ps = sbelow ? 31 - __clz(sbelow) : 0;
+            const int ps_op = __shfl_sync(kFull, op, ps);
+            const uint32_t prev_start = sbelow ? c0 + uint32_t(ps) : run_start;
+            const int prev_run_op = sbelow ? ps_op : run_op;
+            const bool close_prev = start && prev_run_op >= 0;
+            const uint32_t close_len = c - prev_start;
+            int tl = 0;
+            if (close_prev) tl += decimal_digits(close_len) + 1;
+            if (start && ins > 0) tl += decimal_digits(uint32_t(ins)) + 1;
+            int x = tl;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int y = __shfl_up_sync(kFull, x, d);
+                if (lane >= d) x += y;
+            }
+            const int total = __shfl_sync(kFull, x, 31);
+            if (write && tl) {
+                int at = int(pos) + x - tl;
+                if (close_prev) at = put_run(dst, at, true, int(close_len), prev_run_op ? 'D' : 'M');
+                if (ins > 0) put_run(dst, at, true, ins, 'I');
+            }
+            pos += uint64_t(total);
+            if (sm) {
+                const int hs = 31 - __clz(sm);
+                run_start = c0 + uint32_t(hs);
+                run_op = __shfl_sync(kFull, op, hs);
+            }
+            const int last_lane = int(min(31u, n - 1 - c0));
+            carry_op = __shfl_sync(kFull, op, last_lane);
+            if (mm) carry_v = __shfl_sync(kFull, v, 31 - __clz(mm));
+        }
+        // the open run, then the query positions after the last match
+        const uint32_t last_len = n - run_start;
+        const int tail = int(P.m) - 1 - carry_v;
+        uint64_t end = pos + decimal_digits(last_len) + 1;
+        if (tail > 0) end += decimal_digits(uint32_t(tail)) + 1;
+        if (lane == 0) {
+            if (write) {
+                const int at = put_run(dst, int(pos), true, int(last_len), run_op ? 'D' : 'M');
+                if (tail > 0) put_run(dst, at, true, tail, 'I');
+            } else {
+                lens[i] = end;
+            }
         }
     }
-    const int tail = int(P.m) - 1 - qprev;
-    if (tail > 0) emit('I', tail);
-    if (run_len > 0) pos = put_run(dst, pos, write != 0, run_len, run_op);
-    if (!write) lens[i] = uint64_t(pos);
 }
 
 __global__ void exclusive_scan_kernel(const uint64_t* in, uint64_t* out, uint32_t n) {
@@ -1292,12 +1371,13 @@ void NwEngine::run() {
         ntasks = h_cnt[1];
         cur ^= 1;
     }
-    nw_breakpoints_kernel<<<int((n + 127) / 128), 128, 0, stream_>>>(a);
+    const int warp_grid = int(std::max<size_t>(1, std::min<size_t>((n + 7) / 8, size_t(dev_.sm_count) * 16)));
+    nw_breakpoints_kernel<<<warp_grid, 256, 0, stream_>>>(a);
     ++stats_.launches;
     if (want_cigar_) {
         d_ciglen_.reserve((n + 1) * sizeof(uint64_t));
         d_cigoff_.reserve((n + 1) * sizeof(uint64_t));
-        nw_cigar_kernel<<<int((n + 127) / 128), 128, 0, stream_>>>(a, d_ciglen_.as<uint64_t>(), nullptr,
+        nw_cigar_kernel<<<warp_grid, 256, 0, stream_>>>(a, d_ciglen_.as<uint64_t>(), nullptr,
                                                                    nullptr, 0);
         exclusive_scan_kernel<<<1, 1024, 0, stream_>>>(d_ciglen_.as<uint64_t>(), d_cigoff_.as<uint64_t>(),
                                                        uint32_t(n));
@@ -1306,7 +1386,7 @@ void NwEngine::run() {
                    "D2H cigar total");
         check_cuda(cudaStreamSynchronize(stream_), "sync cigar");
         d_cig_.reserve(std::max<uint64_t>(total, 1));
-        nw_cigar_kernel<<<int((n + 127) / 128), 128, 0, stream_>>>(a, d_ciglen_.as<uint64_t>(),
+        nw_cigar_kernel<<<warp_grid, 256, 0, stream_>>>(a, d_ciglen_.as<uint64_t>(),
                                                                    d_cigoff_.as<uint64_t>(), d_cig_.as<char>(), 1);
         stats_.launches += 4;
     }
