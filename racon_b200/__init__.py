@@ -253,6 +253,24 @@ class Context:
             out.append({"edit_distance": r.edit_distance[i], "breakpoints": bp, "cigar": cig})
         return out
 
+    def prepare_pairs(self, pairs):
+        """The rb_pair array (host buffers) for pairs, to pass to
+        align_prepared repeatedly."""
+        arr, keep = self._pairs(pairs)
+        return arr, keep, len(pairs)
+
+    def align_prepared(self, prepared, want_cigar=True):
+        """rb_align_batch on a prepare_pairs array; returns the raw result
+        (library-owned arrays) without converting it to Python objects."""
+        arr, _, n = prepared
+        r = _AlnResult()
+        self._check(self.lib.rb_align_batch(self.ptr, arr, n, int(want_cigar), ctypes.byref(r)))
+        return r
+
+    def aln_results(self, r, n, want_cigar=True):
+        """Python view of a raw rb_aln_result of n pairs."""
+        return self._aln_out(r, n, want_cigar)
+
     def align(self, pairs, want_cigar=True):
         """pairs: list of dicts with query, target, q_offset, t_begin."""
         arr, keep = self._pairs(pairs)

@@ -48,6 +48,8 @@
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <thread>
+#include <vector>
 
 #include "rb_internal.hpp"
 
@@ -1107,10 +1109,10 @@ NwEngine::~NwEngine() {
 void NwEngine::stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t window_length) {
     if (n > 0 && !pairs) throw Error{RB_ERR_ARG, "rb_align: pairs is NULL"};
     if (window_length == 0) throw Error{RB_ERR_ARG, "rb_align: window length is 0"};
-    npairs_ = n;
+    npairs_ = 0;
     want_cigar_ = want_cigar;
     window_length_ = window_length;
-    // pack: per-pair symbol numbering by first appearance, query then target
+    // sizes and offsets (16-byte aligned per sequence)
     uint64_t bytes = 0, mq_len = 0, bp_slots = 0;
     max_m_ = max_n_ = 0;
     for (size_t i = 0; i < n; ++i) {
@@ -1135,31 +1137,23 @@ void NwEngine::stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t wi
     h_codes_.reserve(std::max<uint64_t>(bytes, 16));
     h_pairs_.reserve(std::max<size_t>(n, 1) * sizeof(NwPairDev));
     h_order_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
+    h_src_.reserve(std::max<size_t>(n, 1) * sizeof(NwStoreSrc));
     uint8_t* codes = h_codes_.as<uint8_t>();
     NwPairDev* pd = h_pairs_.as<NwPairDev>();
+    NwStoreSrc* src = h_src_.as<NwStoreSrc>();
+    // raw bytes go to the device as they are; nw_encode_kernel numbers each
+    // pair's symbols there, in place
     uint64_t off = 0, mqo = 0, bpo = 0;
-    int16_t map[256];
     for (size_t i = 0; i < n; ++i) {
         const rb_pair& p = pairs[i];
-        std::fill(map, map + 256, int16_t(-1));
-        int nsym = 0;
         NwPairDev& d = pd[i];
         d.q_off = off;
-        for (uint32_t k = 0; k < p.query_length; ++k) {
-            const uint8_t ch = uint8_t(p.query[k]);
-            if (map[ch] < 0) map[ch] = int16_t(nsym++);
-            codes[off + k] = uint8_t(map[ch]);
-        }
         off += (p.query_length + 15) & ~15u;
         d.t_off = off;
-        for (uint32_t k = 0; k < p.target_length; ++k) {
-            const uint8_t ch = uint8_t(p.target[k]);
-            if (map[ch] < 0) map[ch] = int16_t(nsym++);
-            codes[off + k] = uint8_t(map[ch]);
-        }
         off += (p.target_length + 15) & ~15u;
-        if (nsym > kMaxSym) throw Error{RB_ERR_ARG, "rb_align: more than 32 distinct symbols in a pair"};
-        d.nsym = uint32_t(std::max(nsym, 1));
+        src[i].q_src = d.q_off;
+        src[i].t_src = d.t_off;
+        d.nsym = 1;
         d.m = p.query_length;
         d.n = p.target_length;
         d.mq_off = mqo;
@@ -1172,6 +1166,20 @@ void NwEngine::stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t wi
         }
         d.q_offset = p.q_offset;
         d.t_begin = p.t_begin;
+    }
+    auto copy_range = [&](size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) {
+            if (pairs[i].query_length) memcpy(codes + pd[i].q_off, pairs[i].query, pairs[i].query_length);
+            if (pairs[i].target_length) memcpy(codes + pd[i].t_off, pairs[i].target, pairs[i].target_length);
+        }
+    };
+    const unsigned nth = bytes > (uint64_t(64) << 20) ? std::max(1u, std::min(8u, std::thread::hardware_concurrency())) : 1u;
+    if (nth == 1) {
+        copy_range(0, n);
+    } else {
+        std::vector<std::thread> pool;
+        for (unsigned k = 0; k < nth; ++k) pool.emplace_back(copy_range, n * k / nth, n * (k + 1) / nth);
+        for (auto& th : pool) th.join();
     }
     // size-sorted work order: largest banded work first
     uint32_t* order = h_order_.as<uint32_t>();
@@ -1188,18 +1196,33 @@ void NwEngine::stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t wi
     d_bp_.reserve(std::max<uint64_t>(bp_slots, 1) * sizeof(uint32_t));
     d_bpcnt_.reserve(std::max<size_t>(n, 1) * sizeof(uint32_t));
     d_misc_.reserve(64);
+    d_src_.reserve(std::max<size_t>(n, 1) * sizeof(NwStoreSrc));
     check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
-    check_cuda(cudaMemcpyAsync(d_codes_.ptr, codes, bytes, cudaMemcpyHostToDevice, stream_), "H2D codes");
+    check_cuda(cudaMemcpyAsync(d_codes_.ptr, codes, bytes, cudaMemcpyHostToDevice, stream_), "H2D sequences");
     check_cuda(cudaMemcpyAsync(d_pairs_.ptr, pd, n * sizeof(NwPairDev), cudaMemcpyHostToDevice, stream_),
                "H2D pairs");
     check_cuda(cudaMemcpyAsync(d_order_.ptr, order, n * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_),
                "H2D order");
+    unsigned int status = 0;
+    if (n) {
+        check_cuda(cudaMemcpyAsync(d_src_.ptr, src, n * sizeof(NwStoreSrc), cudaMemcpyHostToDevice, stream_),
+                   "H2D pair sources");
+        check_cuda(cudaMemsetAsync(d_misc_.ptr, 0, 64, stream_), "memset status");
+        const int grid = int(std::max<size_t>(1, std::min<size_t>((n + 7) / 8, size_t(dev_.sm_count) * 8)));
+        nw_encode_kernel<<<grid, 256, 0, stream_>>>(d_codes_.as<uint8_t>(), d_src_.as<NwStoreSrc>(),
+                                                    d_pairs_.as<NwPairDev>(), d_codes_.as<uint8_t>(), uint32_t(n),
+                                                    d_misc_.as<unsigned int>());
+        check_cuda(cudaGetLastError(), "nw_encode_kernel");
+        check_cuda(cudaMemcpyAsync(&status, d_misc_.ptr, 4, cudaMemcpyDeviceToHost, stream_), "D2H status");
+    }
     check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
     check_cuda(cudaStreamSynchronize(stream_), "stage sync");
+    if (status) throw Error{RB_ERR_ARG, "rb_align: more than 32 distinct symbols in a pair"};
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0_, ev1_);
     stats_.h2d_ms = ms;
-    stats_.h2d_bytes = bytes + n * (sizeof(NwPairDev) + sizeof(uint32_t));
+    stats_.h2d_bytes = bytes + n * (sizeof(NwPairDev) + sizeof(NwStoreSrc) + sizeof(uint32_t));
+    npairs_ = n;
 }
 
 void NwEngine::stage_store(const rb_store_pair* pairs, size_t n, int want_cigar, uint32_t window_length,
