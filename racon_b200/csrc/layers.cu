@@ -386,11 +386,30 @@ void LayerEngine::stage_sequences(const rb_sequence* seqs, size_t n, PoaEngine& 
     }
     h_store_.reserve(std::max<uint64_t>(up, 16));
     uint8_t* h = h_store_.as<uint8_t>();
-    for (size_t i = 0; i < n; ++i) {
-        const SeqDev& d = tab[i];
-        if (d.fwd == kNone) continue;
-        if (d.len) memcpy(h + d.fwd, seqs[i].data, d.len);
-        if (d.fq != kNone && d.len) memcpy(h + d.fq, seqs[i].quality, d.len);
+    auto copy_range = [&](size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) {
+            const SeqDev& d = tab[i];
+            if (d.fwd == kNone || d.len == 0) continue;
+            memcpy(h + d.fwd, seqs[i].data, d.len);
+            if (d.fq != kNone) memcpy(h + d.fq, seqs[i].quality, d.len);
+        }
+    };
+    const unsigned nth = up > (uint64_t(32) << 20) ? std::max(1u, std::min(8u, std::thread::hardware_concurrency())) : 1u;
+    if (nth == 1) {
+        copy_range(0, n);
+    } else {
+        // ranges of about equal bytes
+        std::vector<std::thread> pool;
+        size_t b = 0;
+        for (unsigned k = 0; k < nth && b < n; ++k) {
+            const uint64_t goal = up * (k + 1) / nth;
+            size_t e = b;
+            while (e < n && (k + 1 == nth || tab[e].fwd == kNone || tab[e].fwd < goal)) ++e;
+            pool.emplace_back(copy_range, b, e);
+            b = e;
+        }
+        if (b < n) copy_range(b, n);
+        for (auto& th : pool) th.join();
     }
     d_store_.reserve(std::max<uint64_t>(dev_bytes, 16));
     d_seqs_.reserve(std::max<size_t>(n, 1) * sizeof(SeqDev));

@@ -1505,13 +1505,17 @@ void NwEngine::fetch(rb_aln_result* out) {
     const size_t n = npairs_;
     check_cuda(cudaEventRecord(ev2_, stream_), "cudaEventRecord");
     dist_.resize(n);
-    std::vector<uint32_t> cnt(n);
-    std::vector<uint32_t> raw(bp_slots_);
+    // pinned staging: the breakpoint slots and counts, and the CIGAR text,
+    // which the result points into directly
+    h_bpcnt_.reserve(std::max<size_t>(n, 1) * 4);
+    h_bp_.reserve(std::max<uint64_t>(bp_slots_, 1) * 4);
+    const uint32_t* cnt = h_bpcnt_.as<uint32_t>();
+    const uint32_t* raw = h_bp_.as<uint32_t>();
     if (n) {
         check_cuda(cudaMemcpyAsync(dist_.data(), d_dist_.ptr, n * 4, cudaMemcpyDeviceToHost, stream_), "D2H dist");
-        check_cuda(cudaMemcpyAsync(cnt.data(), d_bpcnt_.ptr, n * 4, cudaMemcpyDeviceToHost, stream_), "D2H bpcnt");
+        check_cuda(cudaMemcpyAsync(h_bpcnt_.ptr, d_bpcnt_.ptr, n * 4, cudaMemcpyDeviceToHost, stream_), "D2H bpcnt");
         if (bp_slots_)
-            check_cuda(cudaMemcpyAsync(raw.data(), d_bp_.ptr, bp_slots_ * 4, cudaMemcpyDeviceToHost, stream_),
+            check_cuda(cudaMemcpyAsync(h_bp_.ptr, d_bp_.ptr, bp_slots_ * 4, cudaMemcpyDeviceToHost, stream_),
                        "D2H bp");
     }
     uint64_t d2h = n * 8 + bp_slots_ * 4;
@@ -1521,9 +1525,9 @@ void NwEngine::fetch(rb_aln_result* out) {
         check_cuda(cudaMemcpyAsync(cigoff.data(), d_cigoff_.ptr, (n + 1) * 8, cudaMemcpyDeviceToHost, stream_),
                    "D2H cigoff");
         check_cuda(cudaStreamSynchronize(stream_), "sync fetch");
-        cig_.resize(cigoff[n]);
+        h_cig_.reserve(std::max<uint64_t>(cigoff[n], 1));
         if (cigoff[n])
-            check_cuda(cudaMemcpyAsync(cig_.data(), d_cig_.ptr, cigoff[n], cudaMemcpyDeviceToHost, stream_),
+            check_cuda(cudaMemcpyAsync(h_cig_.ptr, d_cig_.ptr, cigoff[n], cudaMemcpyDeviceToHost, stream_),
                        "D2H cigars");
         d2h += (n + 1) * 8 + cigoff[n];
     }
@@ -1539,7 +1543,7 @@ void NwEngine::fetch(rb_aln_result* out) {
     bp_.clear();
     for (size_t i = 0; i < n; ++i) {
         bp_offsets_[i] = bp_.size();
-        bp_.insert(bp_.end(), raw.begin() + pd[i].bp_off, raw.begin() + pd[i].bp_off + cnt[i]);
+        bp_.insert(bp_.end(), raw + pd[i].bp_off, raw + pd[i].bp_off + cnt[i]);
     }
     bp_offsets_[n] = bp_.size();
     out->edit_distance = dist_.data();
@@ -1547,7 +1551,8 @@ void NwEngine::fetch(rb_aln_result* out) {
     out->bp_offsets = bp_offsets_.data();
     if (want_cigar_) {
         cig_offsets_ = cigoff.empty() ? std::vector<uint64_t>(n + 1, 0) : cigoff;
-        out->cigars = cig_.data();
+        if (cigoff.empty()) h_cig_.reserve(1);
+        out->cigars = h_cig_.as<char>();
         out->cigar_offsets = cig_offsets_.data();
     } else {
         out->cigars = nullptr;

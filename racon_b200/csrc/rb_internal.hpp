@@ -114,7 +114,6 @@ private:
     std::vector<int32_t> dist_;
     std::vector<uint64_t> bp_offsets_, cig_offsets_;
     std::vector<uint32_t> bp_;
-    std::vector<char> cig_;
     rb_stats stats_{};
 };
 
