@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <thread>
@@ -485,8 +486,11 @@ void LayerEngine::assemble_aligned(size_t n_targets, const rb_store_pair* pairs,
         out_bp_off_.assign(1, 0);
     }
     const SeqStore st = store();
-    // batches bounded by bases so the aligner's buffers stay modest
-    const uint64_t kBatchBases = uint64_t(1) << 31;
+    // batches bounded by bases so the aligner's buffers stay modest;
+    // RB_ALIGN_BATCH_BASES lowers the bound (tests of the multi-batch path);
+    // results do not depend on it
+    uint64_t kBatchBases = uint64_t(1) << 31;
+    if (const char* e = getenv("RB_ALIGN_BATCH_BASES")) kBatchBases = std::max<uint64_t>(1, strtoull(e, nullptr, 10));
     std::vector<OvlDev> od;
     size_t b = 0;
     while (b < n) {

@@ -141,3 +141,21 @@ def test_fused_staging_matches_two_steps(native_lib, seed):
         ctx.poa_run()
         assert ctx.poa_fetch() == want
         assert any(c != "" for c, _ in want)
+
+
+def test_fused_staging_in_many_alignment_batches(native_lib, monkeypatch):
+    # the aligner runs in batches bounded by bases; every batch's breaking
+    # points go to the layer candidates in overlap order
+    seqs, pairs = _world(8, n_reads=50)
+    with native_lib.Context(0, 3, -5, -4, 500) as ctx:
+        ctx.sequences_stage(seqs)
+        want_aln = ctx.poa_stage_alignments(2, pairs, quality_threshold=10.0, tgs=True)
+        ctx.poa_run()
+        want = ctx.poa_fetch()
+        monkeypatch.setenv("RB_ALIGN_BATCH_BASES", "6000")
+        got_aln = ctx.poa_stage_alignments(2, pairs, quality_threshold=10.0, tgs=True)
+        ctx.poa_run()
+        got = ctx.poa_fetch()
+        assert ctx.layer_stats().launches > 20  # one candidates launch per batch
+    assert got_aln == want_aln
+    assert got == want
