@@ -250,7 +250,12 @@ def run_serving(args, device, rates):
             span = max(r[1]["finished"] for r in res) - min(r[1]["submitted"] for r in res)
             return [r[0] for r in res], [r[1] for r in res], span
 
-        run(None)  # warm: every worker's device buffers reach their working size
+        run(None)  # warm-up pass
+        # every worker's buffers at the working size: the largest job once per
+        # worker, all at once (an idle worker takes each)
+        big = max(range(len(jobs)), key=lambda i: windows[i])
+        for t in [srv.submit(*jobs[big][:3]) for _ in range(args.workers)]:
+            srv.wait(t)
         iso, alone = [], []
         for j in jobs:
             fasta, tm = srv.wait(srv.submit(j[0], j[1], j[2]))

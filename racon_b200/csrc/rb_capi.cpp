@@ -20,15 +20,41 @@ void check_cuda(cudaError_t e, const char* what) {
     }
 }
 
+namespace {
+thread_local cudaStream_t t_alloc_stream = nullptr;
+thread_local bool t_alloc_bound = false;
+}  // namespace
+
+AllocStreamScope::AllocStreamScope(cudaStream_t s) : prev(t_alloc_stream), prev_bound(t_alloc_bound) {
+    t_alloc_stream = s;
+    t_alloc_bound = true;
+}
+AllocStreamScope::~AllocStreamScope() {
+    t_alloc_stream = prev;
+    t_alloc_bound = prev_bound;
+}
+
 void DevBuf::reserve(size_t need) {
     if (need <= bytes && ptr) return;
     release();
     size_t b = need < 256 ? 256 : need;
-    check_cuda(cudaMalloc(&ptr, b), "cudaMalloc");
+    if (t_alloc_bound) {
+        check_cuda(cudaMallocAsync(&ptr, b, t_alloc_stream), "cudaMallocAsync");
+        stream = t_alloc_stream;
+        stream_ordered = true;
+    } else {
+        check_cuda(cudaMalloc(&ptr, b), "cudaMalloc");
+        stream_ordered = false;
+    }
     bytes = b;
 }
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        if (stream_ordered)
+            cudaFreeAsync(ptr, stream);
+        else
+            cudaFree(ptr);
+    }
     ptr = nullptr;
     bytes = 0;
 }
@@ -78,6 +104,7 @@ int guarded(rb_ctx* ctx, F&& f) {
     if (!ctx) return RB_ERR_ARG;
     try {
         cudaSetDevice(ctx->dev.device);
+        rb::AllocStreamScope scope(ctx->stream);
         f();
         ctx->err.clear();
         return RB_OK;

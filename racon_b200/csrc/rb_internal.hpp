@@ -21,10 +21,14 @@ struct Error {
 
 void check_cuda(cudaError_t e, const char* what);
 
-// Growable device buffer (cudaMalloc'd, reused across calls).
+// Growable device buffer, reused across calls. Inside a C ABI call it grows
+// in the calling context's stream order (cudaMallocAsync / cudaFreeAsync), so
+// growing never waits for other contexts' work on the device.
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;  // stream of the allocation when stream-ordered
+    bool stream_ordered = false;
     void reserve(size_t need);
     void release();
     template <class T> T* as() const { return static_cast<T*>(ptr); }
@@ -39,6 +43,15 @@ struct HostBuf {
     void release();
     template <class T> T* as() const { return static_cast<T*>(ptr); }
     ~HostBuf() { release(); }
+};
+
+// Binds the calling thread's device-buffer growth to a context's stream for
+// the duration of one C ABI call (rb_capi.cpp).
+struct AllocStreamScope {
+    explicit AllocStreamScope(cudaStream_t s);
+    ~AllocStreamScope();
+    cudaStream_t prev;
+    bool prev_bound;
 };
 
 struct DeviceInfo {
