@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Throughput of racon's polishing hot path on B200: window POA consensus.
 
-Workload (BASELINE configuration "batched POA + edlib on GPU"): seeded
+Workload (the batched POA + edlib configuration, config 1): seeded
 synthetic 1 Mb genome, draft with 1% errors, 50x FASTQ reads (log-normal
 8 kb / 4 kb, 12% error, Phred U[5,30]), PAF from true coordinates with +-50 bp
 end jitter, racon defaults -w 500 -m 3 -x -5 -g -4 -q 10 -e 0.3. racon's
@@ -16,7 +16,9 @@ untimed; a step is the consensus of every window of the job.
          device from the breaking points; rb_poa_run; rb_poa_fetch)
   e2e_host_layers  the same through rb_poa_batch with host-assembled
          windows (pack every layer's bases, H2D, kernels, D2H, unpack)
-  roofline / compute  see DESIGN.md (the POA DP is integer-issue bound)
+  roofline / compute  HBM bytes (bases and qualities in, consensus out) and
+         int32 issue (about 6 ops per DP cell) of poa_kernel; the POA DP is
+         integer-issue bound
   cpu_baseline  the CPU oracle (restatement of racon's algorithm, not
          reference racon, which does not build here) on a bounded sample of
          the same windows with every host thread
