@@ -255,6 +255,18 @@ int rb_align_stage(rb_ctx* ctx, const rb_pair* pairs, size_t n, int want_cigar);
 int rb_align_run(rb_ctx* ctx);
 int rb_align_fetch(rb_ctx* ctx, rb_aln_result* out);
 
+/* Scheduling of a context's kernels, for callers that run several contexts
+ * on one device at once (the serving loop); results do not depend on either.
+ * rb_set_yield: windows a warp of the consensus kernel, and pairs or
+ * Hirschberg tasks a warp of the alignment kernels, take per launch (0, the
+ * default: the kernels are persistent until their work queue is empty). Small
+ * values make the kernels of a large job return SMs at every launch boundary,
+ * where other contexts' waiting kernels can take them.
+ * rb_set_priority: 1 puts the context's work on a stream of the highest
+ * priority, 0 on a normal one (between calls). */
+int rb_set_yield(rb_ctx* ctx, uint32_t consensus_windows, uint32_t alignment_items);
+int rb_set_priority(rb_ctx* ctx, int high);
+
 /* Counters of the last run/batch call of each kind. */
 typedef struct rb_stats {
     double kernel_ms;        /* device time of the compute kernels (CUDA events) */

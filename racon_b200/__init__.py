@@ -154,6 +154,8 @@ def load():
                                             ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                             ctypes.POINTER(_AlnResult)]
     lib.rb_layer_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    lib.rb_set_yield.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
+    lib.rb_set_priority.argtypes = [vp, ctypes.c_int]
     lib.rb_sequence_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.rb_job_layer_input.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(_Sequence)),
                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
@@ -459,6 +461,14 @@ class Context:
         s = Stats()
         self._check(self.lib.rb_sequence_stats(self.ptr, ctypes.byref(s)))
         return s
+
+    def set_yield(self, consensus_windows, alignment_items):
+        """Work a warp takes per launch (0: persistent kernels); rb_set_yield."""
+        self._check(self.lib.rb_set_yield(self.ptr, consensus_windows, alignment_items))
+
+    def set_priority(self, high):
+        """High- or normal-priority stream for this context; rb_set_priority."""
+        self._check(self.lib.rb_set_priority(self.ptr, int(high)))
 
     def poa_stats(self):
         s = Stats()

@@ -3,13 +3,16 @@
 // of device contexts alive and runs jobs as they arrive.
 //
 // Design:
-//   - `workers` threads, each owning one rb_ctx (own CUDA stream, own device
+//   - `workers` threads, each owning one rb_ctx (own CUDA streams, own device
 //     buffers). Buffers grow to the largest job a worker has run and stay
-//     allocated, so a steady stream of jobs does no cudaMalloc / cudaFree
-//     (which would synchronise the device and stall the other workers).
+//     allocated; growth is stream-ordered, so it does not synchronise the
+//     device under the other workers.
 //   - Jobs on different workers overlap on the device: one job's host stages
 //     (parsing, layer assembly, stitching) run while another's kernels run,
-//     and the kernels of concurrent jobs share the SMs as CTAs retire.
+//     and the kernels of concurrent jobs share the SMs as CTAs retire. (The
+//     contexts' kernels stay persistent: bounded work per launch with small
+//     jobs on the high-priority stream, rb_set_yield / rb_set_priority, made
+//     isolated jobs slower and the p99 latency ratio no better.)
 //   - Admission is first in first out by estimated device footprint: the
 //     head of the queue starts when a worker is idle and its estimate fits
 //     beside the jobs in flight within hbm_budget (a job alone always

@@ -98,6 +98,7 @@ struct NwDevArgs {
     uint32_t ntasks_in;
     NwTask* tasks_out;
     uint32_t tasks_out_cap;
+    uint32_t per_warp_cap;   // pairs / tasks a warp takes per launch (0: until the queue is empty)
 };
 
 __device__ __forceinline__ int fdiv64(int a) { return a >= 0 ? a / 64 : -((-a + 63) / 64); }
@@ -581,7 +582,7 @@ nw_distance_kernel(NwDevArgs a) {
     const uint32_t slot = blockIdx.x * kWarpsPerBlock + wib;
     u64* peq = g_peq_smem + wib * kMaxSym * 32;
     const WarpScratch ws = warp_scratch(a, slot);
-    while (true) {
+    for (uint32_t done = 0; a.per_warp_cap == 0 || done < a.per_warp_cap; ++done) {
         unsigned i = 0;
         if (lane == 0) i = atomicAdd(&a.counters[0], 1u);
         i = __shfl_sync(kFull, i, 0);
@@ -635,7 +636,7 @@ nw_level_kernel(NwDevArgs a) {
     const uint32_t slot = blockIdx.x * kWarpsPerBlock + wib;
     u64* peq = g_peq_smem + wib * kMaxSym * 32;
     const WarpScratch ws = warp_scratch(a, slot);
-    while (true) {
+    for (uint32_t done = 0; a.per_warp_cap == 0 || done < a.per_warp_cap; ++done) {
         unsigned i = 0;
         if (lane == 0) i = atomicAdd(&a.counters[0], 1u);
         i = __shfl_sync(kFull, i, 0);
@@ -1364,8 +1365,17 @@ void NwEngine::run() {
     const size_t smem = kWarpsPerBlock * kMaxSym * 32 * 8;
     check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
     check_cuda(cudaMemsetAsync(a.counters, 0, 64, stream_), "memset counters");
-    nw_distance_kernel<<<grid, 32 * kWarpsPerBlock, smem, stream_>>>(a);
-    ++stats_.launches;
+    // persistent by default; with a per-warp cap, enough launches back to
+    // back that every pair (task) is taken
+    a.per_warp_cap = yield_items_;
+    auto launches_for = [&](size_t items) {
+        return yield_items_ ? (items + scratch_warps_ * yield_items_ - 1) / (scratch_warps_ * yield_items_)
+                            : size_t(1);
+    };
+    for (size_t l = launches_for(n); l > 0; --l) {
+        nw_distance_kernel<<<grid, 32 * kWarpsPerBlock, smem, stream_>>>(a);
+        ++stats_.launches;
+    }
     // level 0 tasks
     a.tasks_out = d_tasks_[0].as<NwTask>();
     a.tasks_out_cap = uint32_t(task_cap);
@@ -1386,8 +1396,10 @@ void NwEngine::run() {
         a.tasks_out = d_tasks_[cur ^ 1].as<NwTask>();
         a.tasks_out_cap = uint32_t(task_cap);
         check_cuda(cudaMemsetAsync(a.counters, 0, 8, stream_), "memset counters");
-        nw_level_kernel<<<grid, 32 * kWarpsPerBlock, smem, stream_>>>(a);
-        ++stats_.launches;
+        for (size_t l = launches_for(ntasks); l > 0; --l) {
+            nw_level_kernel<<<grid, 32 * kWarpsPerBlock, smem, stream_>>>(a);
+            ++stats_.launches;
+        }
         check_cuda(cudaMemcpyAsync(h_cnt, a.counters, 16, cudaMemcpyDeviceToHost, stream_), "D2H count");
         check_cuda(cudaStreamSynchronize(stream_), "sync level");
         if (h_cnt[2] != 0) throw Error{RB_ERR_DEVICE, "nw: level kernel status " + std::to_string(h_cnt[2])};

@@ -72,6 +72,7 @@ struct PoaArgs {
     int trim;
     unsigned int* counters;      // [0] window cursor, [1] status
     unsigned long long* cells;   // DP cells computed
+    uint32_t per_warp_cap;       // windows a warp takes per launch (0: until the queue is empty)
 };
 
 // Per-slot scratch view.
@@ -2329,7 +2330,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) poa_kernel(PoaA
     if (lane == 0) g_all[wid] = make_graph(a, slot);
     __syncwarp();
     const Graph& g = g_all[wid];
-    while (true) {
+    // with a cap the CTA retires after that many windows per warp, so other
+    // streams' kernels get SMs between launches (the host launches enough)
+    for (uint32_t done = 0; a.per_warp_cap == 0 || done < a.per_warp_cap; ++done) {
         unsigned k = 0;
         if (lane == 0) k = atomicAdd(&a.counters[0], 1u);
         k = __shfl_sync(0xffffffffu, k, 0);
@@ -2655,8 +2658,17 @@ void PoaEngine::run(bool plain) {
             const int smem = kWarpsPerCta * kRingBytesPerWarp;
             check_cuda(cudaFuncSetAttribute(poa_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                        "cudaFuncSetAttribute");
-            poa_kernel<<<int(slots / kWarpsPerCta), 32 * kWarpsPerCta, smem, stream_>>>(a);
-            ++stats_.launches;
+            // persistent by default; with a per-warp cap, enough launches
+            // back to back that every window is taken
+            size_t launches = 1;
+            if (yield_windows_ > 0) {
+                a.per_warp_cap = yield_windows_;
+                launches = (todo.size() + slots * yield_windows_ - 1) / (slots * yield_windows_);
+            }
+            for (size_t l = 0; l < launches; ++l) {
+                poa_kernel<<<int(slots / kWarpsPerCta), 32 * kWarpsPerCta, smem, stream_>>>(a);
+                ++stats_.launches;
+            }
         }
         check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
         unsigned long long cells = 0;

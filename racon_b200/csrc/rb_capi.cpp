@@ -76,7 +76,9 @@ void HostBuf::release() {
 
 struct rb_ctx {
     rb::DeviceInfo dev;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // the one the engines use now
+    cudaStream_t stream_lo = nullptr;  // normal priority
+    cudaStream_t stream_hi = nullptr;  // highest priority
     rb_params params{};
     std::unique_ptr<rb::NwEngine> nw;
     std::unique_ptr<rb::PoaEngine> poa;
@@ -158,7 +160,12 @@ rb_ctx* rb_create(int device, const rb_params* params) {
     ctx->params = *params;
     try {
         rb::check_cuda(cudaSetDevice(device), "cudaSetDevice");
-        rb::check_cuda(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        rb::check_cuda(cudaStreamCreateWithFlags(&ctx->stream_lo, cudaStreamNonBlocking), "cudaStreamCreate");
+        int least = 0, greatest = 0;
+        rb::check_cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
+        rb::check_cuda(cudaStreamCreateWithPriority(&ctx->stream_hi, cudaStreamNonBlocking, greatest),
+                       "cudaStreamCreateWithPriority");
+        ctx->stream = ctx->stream_lo;
         ctx->nw.reset(new rb::NwEngine(ctx->dev, ctx->stream));
         ctx->poa.reset(new rb::PoaEngine(ctx->dev, ctx->stream, params->match, params->mismatch, params->gap));
         ctx->layers.reset(new rb::LayerEngine(ctx->dev, ctx->stream));
@@ -180,7 +187,8 @@ void rb_destroy(rb_ctx* ctx) {
     ctx->nw.reset();
     ctx->layers.reset();
     ctx->poa.reset();
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->stream_lo) cudaStreamDestroy(ctx->stream_lo);
+    if (ctx->stream_hi) cudaStreamDestroy(ctx->stream_hi);
     delete ctx;
 }
 
@@ -265,6 +273,25 @@ int rb_sequence_stats(const rb_ctx* ctx, rb_stats* out) {
     if (!ctx || !out) return RB_ERR_ARG;
     *out = ctx->layers->sequence_stats();
     return RB_OK;
+}
+
+int rb_set_yield(rb_ctx* ctx, uint32_t consensus_windows, uint32_t alignment_items) {
+    if (!ctx) return RB_ERR_ARG;
+    ctx->poa->set_yield(consensus_windows);
+    ctx->nw->set_yield(alignment_items);
+    return RB_OK;
+}
+int rb_set_priority(rb_ctx* ctx, int high) {
+    return guarded(ctx, [&]() {
+        cudaStream_t s = high ? ctx->stream_hi : ctx->stream_lo;
+        if (s == ctx->stream) return;
+        // every call leaves its stream idle; wait anyway before switching
+        rb::check_cuda(cudaStreamSynchronize(ctx->stream), "stream sync");
+        ctx->stream = s;
+        ctx->nw->set_stream(s);
+        ctx->poa->set_stream(s);
+        ctx->layers->set_stream(s);
+    });
 }
 
 int rb_poa_stats(const rb_ctx* ctx, rb_stats* out) {

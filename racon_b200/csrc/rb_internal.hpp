@@ -101,6 +101,11 @@ public:
     void fetch(rb_aln_result* out);
     // Breaking points of the last run on the device: pair i's (t, q) values
     // at bp_slots()[pairs()[i].bp_off ...], bp_counts()[i] of them.
+    // scheduling (results do not depend on them): the stream the engine
+    // enqueues on, and pairs or tasks a warp takes per launch (0: the
+    // kernels are persistent until their queue is empty)
+    void set_stream(cudaStream_t s) { stream_ = s; }
+    void set_yield(uint32_t items) { yield_items_ = items; }
     const uint32_t* bp_slots() const { return d_bp_.as<uint32_t>(); }
     const uint32_t* bp_counts() const { return d_bpcnt_.as<uint32_t>(); }
     const NwPairDev* pairs() const { return h_pairs_.as<NwPairDev>(); }
@@ -115,6 +120,7 @@ private:
     cudaStream_t stream_;
     cudaEvent_t ev0_, ev1_, ev2_, ev3_;
     size_t npairs_ = 0;
+    uint32_t yield_items_ = 0;
     int want_cigar_ = 0;
     uint32_t window_length_ = 500;
     uint32_t max_m_ = 0, max_n_ = 0;
@@ -170,6 +176,10 @@ public:
                       uint32_t max_len, int trim);
     // Drops a device stage whose buffers are about to change.
     void forget();
+    // scheduling (results do not depend on them): the stream the engine
+    // enqueues on, and windows a warp takes per launch (0: persistent)
+    void set_stream(cudaStream_t s) { stream_ = s; }
+    void set_yield(uint32_t windows) { yield_windows_ = windows; }
     void run(bool plain = false);
     void fetch(rb_poa_result* out);
     const rb_stats& stats() const { return stats_; }
@@ -185,6 +195,7 @@ private:
     cudaEvent_t ev0_, ev1_, ev2_, ev3_;
     int8_t match_, mismatch_, gap_;
     int trim_ = 1;
+    uint32_t yield_windows_ = 0;
     size_t nwin_ = 0;
     uint64_t in_bytes_ = 0, out_cap_ = 0;
     uint32_t max_len_ = 0, max_nodes_cap_ = 0;
@@ -226,6 +237,7 @@ public:
     SeqStore store() const;
     const rb_stats& stats() const { return stats_; }
     const rb_stats& sequence_stats() const { return seq_stats_; }
+    void set_stream(cudaStream_t s) { stream_ = s; }
 
 private:
     void begin(size_t n_targets, uint32_t window_length, double quality_threshold, uint64_t cand_cap);
