@@ -265,6 +265,9 @@ int rb_align_fetch(rb_ctx* ctx, rb_aln_result* out);
  * rb_set_priority: 1 puts the context's work on a stream of the highest
  * priority, 0 on a normal one (between calls). */
 int rb_set_yield(rb_ctx* ctx, uint32_t consensus_windows, uint32_t alignment_items);
+/* Percent of the SMs the context's persistent kernels fill (1..100; 0 or 100:
+ * all), leaving the rest to other contexts' kernels. */
+int rb_set_sm_share(rb_ctx* ctx, uint32_t percent);
 int rb_set_priority(rb_ctx* ctx, int high);
 
 /* Counters of the last run/batch call of each kind. */

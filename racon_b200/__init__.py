@@ -156,6 +156,7 @@ def load():
     lib.rb_layer_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.rb_set_yield.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
     lib.rb_set_priority.argtypes = [vp, ctypes.c_int]
+    lib.rb_set_sm_share.argtypes = [vp, ctypes.c_uint32]
     lib.rb_sequence_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.rb_job_layer_input.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(_Sequence)),
                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
@@ -465,6 +466,10 @@ class Context:
     def set_yield(self, consensus_windows, alignment_items):
         """Work a warp takes per launch (0: persistent kernels); rb_set_yield."""
         self._check(self.lib.rb_set_yield(self.ptr, consensus_windows, alignment_items))
+
+    def set_sm_share(self, percent):
+        """Percent of the SMs the persistent kernels fill; rb_set_sm_share."""
+        self._check(self.lib.rb_set_sm_share(self.ptr, percent))
 
     def set_priority(self, high):
         """High- or normal-priority stream for this context; rb_set_priority."""

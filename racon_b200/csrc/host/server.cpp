@@ -10,9 +10,10 @@
 //   - Jobs on different workers overlap on the device: one job's host stages
 //     (parsing, layer assembly, stitching) run while another's kernels run,
 //     and the kernels of concurrent jobs share the SMs as CTAs retire. (The
-//     contexts' kernels stay persistent: bounded work per launch with small
-//     jobs on the high-priority stream, rb_set_yield / rb_set_priority, made
-//     isolated jobs slower and the p99 latency ratio no better.)
+//     contexts' kernels stay persistent on all SMs: bounded work per launch
+//     with small jobs on the high-priority stream, rb_set_yield /
+//     rb_set_priority, and large jobs on 70 % of the SMs, rb_set_sm_share,
+//     both measured worse for the p99 latency ratio.)
 //   - Admission is first in first out by estimated device footprint: the
 //     head of the queue starts when a worker is idle and its estimate fits
 //     beside the jobs in flight within hbm_budget (a job alone always

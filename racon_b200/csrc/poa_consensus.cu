@@ -2606,7 +2606,10 @@ void PoaEngine::run(bool plain) {
         // resident windows (one warp each): enough to fill the SMs, bounded by
         // a scratch budget
         const size_t budget = scratch_budget_;
-        size_t slots = std::min<size_t>(todo.size(), plain ? todo.size() : size_t(dev_.sm_count) * kWarpsPerCta * kCtasPerSm);
+        // resident windows: the context's share of the SMs (all by default)
+        const size_t resident = std::max<size_t>(
+            kWarpsPerCta, size_t(dev_.sm_count) * kWarpsPerCta * kCtasPerSm * sm_share_pct_ / 100);
+        size_t slots = std::min<size_t>(todo.size(), plain ? todo.size() : resident);
         // RB_POA_SLOTS caps the resident windows (smaller scratch, e.g. for
         // profiler captures); results do not depend on it
         if (const char* e = getenv("RB_POA_SLOTS"))

@@ -281,6 +281,12 @@ int rb_set_yield(rb_ctx* ctx, uint32_t consensus_windows, uint32_t alignment_ite
     ctx->nw->set_yield(alignment_items);
     return RB_OK;
 }
+int rb_set_sm_share(rb_ctx* ctx, uint32_t percent) {
+    if (!ctx || percent > 100) return RB_ERR_ARG;
+    ctx->poa->set_sm_share(percent);
+    ctx->nw->set_sm_share(percent);
+    return RB_OK;
+}
 int rb_set_priority(rb_ctx* ctx, int high) {
     return guarded(ctx, [&]() {
         cudaStream_t s = high ? ctx->stream_hi : ctx->stream_lo;

@@ -106,6 +106,8 @@ public:
     // kernels are persistent until their queue is empty)
     void set_stream(cudaStream_t s) { stream_ = s; }
     void set_yield(uint32_t items) { yield_items_ = items; }
+    // percent of the SMs the persistent kernels fill (100: all)
+    void set_sm_share(uint32_t pct) { sm_share_pct_ = pct ? pct : 100; }
     const uint32_t* bp_slots() const { return d_bp_.as<uint32_t>(); }
     const uint32_t* bp_counts() const { return d_bpcnt_.as<uint32_t>(); }
     const NwPairDev* pairs() const { return h_pairs_.as<NwPairDev>(); }
@@ -121,6 +123,7 @@ private:
     cudaEvent_t ev0_, ev1_, ev2_, ev3_;
     size_t npairs_ = 0;
     uint32_t yield_items_ = 0;
+    uint32_t sm_share_pct_ = 100;
     int want_cigar_ = 0;
     uint32_t window_length_ = 500;
     uint32_t max_m_ = 0, max_n_ = 0;
@@ -180,6 +183,8 @@ public:
     // enqueues on, and windows a warp takes per launch (0: persistent)
     void set_stream(cudaStream_t s) { stream_ = s; }
     void set_yield(uint32_t windows) { yield_windows_ = windows; }
+    // percent of the SMs the persistent kernel fills (100: all)
+    void set_sm_share(uint32_t pct) { sm_share_pct_ = pct ? pct : 100; }
     void run(bool plain = false);
     void fetch(rb_poa_result* out);
     const rb_stats& stats() const { return stats_; }
@@ -196,6 +201,7 @@ private:
     int8_t match_, mismatch_, gap_;
     int trim_ = 1;
     uint32_t yield_windows_ = 0;
+    uint32_t sm_share_pct_ = 100;
     size_t nwin_ = 0;
     uint64_t in_bytes_ = 0, out_cap_ = 0;
     uint32_t max_len_ = 0, max_nodes_cap_ = 0;

@@ -1,6 +1,7 @@
-"""Scheduling knobs of a context (rb_set_yield, rb_set_priority) leave every
-result unchanged: bounded work per warp and launch, with as many launches
-back to back as the queue needs, and the high-priority stream."""
+"""Scheduling knobs of a context (rb_set_yield, rb_set_priority,
+rb_set_sm_share) leave every result unchanged: bounded work per warp and
+launch, with as many launches back to back as the queue needs, the
+high-priority stream, and persistent kernels on part of the SMs."""
 import pytest
 
 from racon_b200 import synthetic
@@ -38,6 +39,12 @@ def test_yield_and_priority_keep_results(native_lib, tmp_path, monkeypatch):
             assert ctx.poa_fetch() == want
             assert ctx.align(pairs, want_cigar=False)[7]["breakpoints"] == want_aln[7]["breakpoints"]
 
+            ctx.set_sm_share(40)
+            assert ctx.align(pairs, want_cigar=True) == want_aln
+            ctx.poa_run()
+            assert ctx.poa_fetch() == want
+
+            ctx.set_sm_share(100)
             ctx.set_priority(False)
             ctx.set_yield(0, 0)
             ctx.poa_run()
