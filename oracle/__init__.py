@@ -47,6 +47,9 @@ def load():
     lib.oracle_dump_windows.restype = c.c_void_p
     lib.oracle_dump_windows.argtypes = [c.c_char_p] * 3 + [c.c_int, c.c_uint32, c.c_double, c.c_double,
                                                            c.c_uint32, c.POINTER(c.c_uint64)]
+    lib.oracle_dump_layer_input.restype = c.c_void_p
+    lib.oracle_dump_layer_input.argtypes = [c.c_char_p] * 3 + [c.c_int, c.c_uint32, c.c_double, c.c_double,
+                                                               c.c_uint32, c.POINTER(c.c_uint64)]
     lib.oracle_free.argtypes = [c.c_void_p]
     lib.oracle_consensus_blob.restype = c.c_int64
     lib.oracle_consensus_blob.argtypes = [c.c_char_p, c.c_uint64, c.c_int64, c.c_uint32, c.c_int, c.c_int, c.c_int,
@@ -125,6 +128,45 @@ def polish(sequences, overlaps, targets, fragment=False, window_length=500, qual
     finally:
         lib.oracle_free(p)
     return text, list(tm), list(cn)
+
+
+def dump_layer_input(sequences, overlaps, targets, fragment=False, window_length=500, quality_threshold=10.0,
+                     error_threshold=0.3, threads=8):
+    """The inputs of racon's layer loop after the breaking points: the
+    sequence table (dicts with data, quality, rc, rquality as bytes or None),
+    the target count, tgs, and the overlaps (q_id, t_id, strand,
+    breakpoints as (t, q) points) in racon's order."""
+    lib = load()
+    nb = ctypes.c_uint64()
+    p = lib.oracle_dump_layer_input(_b(sequences), _b(overlaps), _b(targets), int(fragment), window_length,
+                                    quality_threshold, error_threshold, threads, ctypes.byref(nb))
+    if not p:
+        raise RuntimeError("oracle layer-input dump failed")
+    try:
+        blob = ctypes.string_at(p, nb.value)
+    finally:
+        lib.oracle_free(p)
+    ns, nt, tgs = struct.unpack_from("<QQB", blob, 0)
+    off = 17
+    seqs = []
+    for _ in range(ns):
+        parts = []
+        for _ in range(4):
+            (n,) = struct.unpack_from("<I", blob, off)
+            off += 4
+            parts.append(blob[off:off + n] if n else None)
+            off += n
+        seqs.append({"data": parts[0], "quality": parts[1], "rc": parts[2], "rquality": parts[3]})
+    (no,) = struct.unpack_from("<Q", blob, off)
+    off += 8
+    ovl = []
+    for _ in range(no):
+        q_id, t_id, strand, npts = struct.unpack_from("<IIII", blob, off)
+        off += 16
+        pts = list(struct.iter_unpack("<II", blob[off:off + 8 * npts]))
+        off += 8 * npts
+        ovl.append({"q_id": q_id, "t_id": t_id, "strand": strand, "breakpoints": pts})
+    return {"sequences": seqs, "n_targets": nt, "tgs": bool(tgs), "overlaps": ovl}
 
 
 def dump_windows(sequences, overlaps, targets, fragment=False, window_length=500, quality_threshold=10.0,

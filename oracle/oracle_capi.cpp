@@ -186,6 +186,65 @@ char* oracle_dump_windows(const char* sequences, const char* overlaps, const cha
     return out;
 }
 
+// The inputs of racon's layer loop after initialize()'s breaking points
+// (src/polisher.cpp:401-457), as a binary blob (free with oracle_free), for
+// checking a restatement of that loop against the windows the oracle builds.
+// Layout, little endian: u64 sequences, u64 targets, u8 tgs; per sequence
+// four u32-length-prefixed strings (data, quality, reverse complement,
+// reversed quality; empty when dropped or absent); u64 overlaps; per overlap
+// u32 q_id, u32 t_id, u32 strand, u32 points, then (u32 t, u32 q) per point.
+char* oracle_dump_layer_input(const char* sequences, const char* overlaps, const char* targets,
+                              int fragment, uint32_t window_length, double quality_threshold,
+                              double error_threshold, uint32_t threads, uint64_t* nbytes) {
+    PolishOptions opt;
+    opt.fragment = fragment != 0;
+    opt.window_length = window_length;
+    opt.quality_threshold = quality_threshold;
+    opt.error_threshold = error_threshold;
+    opt.threads = threads;
+    std::vector<CpuSequence> seqs;
+    std::vector<CpuOverlap> ovl;
+    uint64_t targets_n = 0;
+    bool tgs = true;
+    if (collect_layer_input(sequences, overlaps, targets, opt, seqs, targets_n, tgs, ovl)) return nullptr;
+    std::string b;
+    auto put = [&](const void* p, size_t n) { b.append(static_cast<const char*>(p), n); };
+    auto put_str = [&](const std::string& x) {
+        const uint32_t n = uint32_t(x.size());
+        put(&n, 4);
+        put(x.data(), n);
+    };
+    const uint64_t ns = seqs.size();
+    const uint8_t t8 = tgs ? 1 : 0;
+    put(&ns, 8);
+    put(&targets_n, 8);
+    put(&t8, 1);
+    for (const auto& q : seqs) {
+        put_str(q.data);
+        put_str(q.quality);
+        put_str(q.rc);
+        put_str(q.rquality);
+    }
+    const uint64_t no = ovl.size();
+    put(&no, 8);
+    for (const auto& o : ovl) {
+        const uint32_t qid = uint32_t(o.q_id), tid = uint32_t(o.t_id), st = o.strand,
+                       np = uint32_t(o.breaking_points.size());
+        put(&qid, 4);
+        put(&tid, 4);
+        put(&st, 4);
+        put(&np, 4);
+        for (const auto& p : o.breaking_points) {
+            put(&p.first, 4);
+            put(&p.second, 4);
+        }
+    }
+    char* out = static_cast<char*>(malloc(b.size()));
+    memcpy(out, b.data(), b.size());
+    *nbytes = b.size();
+    return out;
+}
+
 }  // extern "C"
 
 #include <atomic>

@@ -743,6 +743,20 @@ int polish_files(const std::string& sp, const std::string& op, const std::string
     return 0;
 }
 
+int collect_layer_input(const std::string& sp, const std::string& op, const std::string& tp,
+                        const PolishOptions& opt, std::vector<CpuSequence>& seqs, uint64_t& n_targets,
+                        bool& tgs, std::vector<CpuOverlap>& overlaps_out) {
+    Loaded L;
+    if (load_inputs(sp, op, tp, opt, L)) return 1;
+    parallel_for(L.overlaps.size(), opt.threads,
+                 [&](uint64_t i) { align_and_break(L.overlaps[i], L.seqs, opt.window_length); });
+    seqs = std::move(L.seqs);
+    n_targets = L.targets;
+    tgs = L.tgs;
+    overlaps_out = std::move(L.overlaps);
+    return 0;
+}
+
 int collect_windows(const std::string& sp, const std::string& op, const std::string& tp,
                     const PolishOptions& opt, std::vector<DumpedWindow>& windows) {
     Loaded L;

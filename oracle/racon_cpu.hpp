@@ -104,6 +104,14 @@ int collect_windows(const std::string& sequences, const std::string& overlaps,
                     const std::string& targets, const PolishOptions& opt,
                     std::vector<DumpedWindow>& windows);
 
+// initialize() up to and including the breaking points: the sequence table
+// (targets first), the target count, racon's window type and the kept
+// overlaps with their breaking points, in racon's order.
+int collect_layer_input(const std::string& sequences, const std::string& overlaps,
+                        const std::string& targets, const PolishOptions& opt,
+                        std::vector<CpuSequence>& seqs, uint64_t& n_targets, bool& tgs,
+                        std::vector<CpuOverlap>& overlaps_out);
+
 // Reads every record of a FASTA/FASTQ file (gzip or plain).
 bool read_sequences(const std::string& path, std::vector<CpuSequence>& out);
 

@@ -10,8 +10,10 @@ Two kinds of cases:
   filter (< 0.02 w), the mean-quality filter at its boundary, add_layer's
   begin == end skip, reverse-strand slicing, reads without qualities, and a
   window with many layers of equal begin (racon's unstable sort). The
-  expected windows come from a restatement of racon's loop below; the
-  library's rb_poa_batch then computes both consensuses.
+  expected windows come from a restatement of racon's loop
+  (tests/layer_loop.py, checked against the oracle's own windows by
+  tests/test_cpu_layer_loop.py); the library's rb_poa_batch then computes
+  both consensuses.
 Quality bytes outside '!'..'~' are refused (RB_ERR_ARG) once they would
 reach a window graph; the filter still reads them with racon's uint32
 wrap-around, so such a layer is kept (and refused) where racon keeps it.
@@ -20,58 +22,17 @@ import random
 
 import pytest
 
+from layer_loop import host_windows, revcomp
 from racon_b200 import RaconB200Error, synthetic
 
 pytestmark = pytest.mark.gpu
 
-COMP = {ord("A"): "T", ord("T"): "A", ord("C"): "G", ord("G"): "C"}
-
-
 def _revcomp(s):
-    return "".join(COMP.get(ord(c), c) for c in reversed(s))
+    return revcomp(s).decode()
 
 
 def _host_windows(seqs, n_targets, overlaps, w, q_thr, tgs):
-    """racon's window creation and layer loop (src/polisher.cpp:384-457)."""
-    windows, first = [], []
-    for t in range(n_targets):
-        first.append(len(windows))
-        d, qd = seqs[t]["data"], seqs[t].get("quality")
-        for r, j in enumerate(range(0, len(d), w)):
-            bl = min(j + w, len(d)) - j
-            windows.append({"backbone": d[j:j + bl], "backbone_quality": qd[j:j + bl] if qd else None,
-                            "layers": [], "qualities": [], "begins": [], "ends": [], "tgs": tgs, "id": t,
-                            "rank": r})
-    for o in overlaps:
-        s = seqs[o["q_id"]]
-        data = _revcomp(s["data"]) if o["strand"] else s["data"]
-        qual = s.get("quality")
-        if qual is not None and o["strand"]:
-            qual = qual[::-1]
-        bp = o["breakpoints"]
-        for j in range(0, len(bp), 2):
-            (t0, q0), (t1, q1) = bp[j], bp[j + 1]
-            if q1 - q0 < 0.02 * w:
-                continue
-            if qual is not None:
-                # (uint32)char - 33 summed into a double: exact integers
-                total = 0
-                for c in qual[q0:q1]:
-                    signed = c - 256 if c >= 128 else c
-                    total += (signed - 33) % (1 << 32)
-                if total / (q1 - q0) < q_thr:
-                    continue
-            win = first[o["t_id"]] + t0 // w
-            ws = (t0 // w) * w
-            b, e = t0 - ws, t1 - ws - 1
-            if b == e:
-                continue
-            W = windows[win]
-            W["layers"].append(data[q0:q1])
-            W["qualities"].append(qual[q0:q1] if qual is not None else None)
-            W["begins"].append(b)
-            W["ends"].append(e)
-    return windows
+    return host_windows(seqs, n_targets, overlaps, w, q_thr, tgs)
 
 
 def _mutate(rng, s, err):
