@@ -305,6 +305,7 @@ std::string PoaGraph::generate_consensus(std::vector<uint32_t>& coverages) {
     return out;
 }
 
+__attribute__((target_clones("avx2", "default")))
 PoaAlignment poa_align_nw(const char* seq, uint32_t len, const PoaGraph& g,
                           int match, int mismatch, int gap, PoaStats* stats) {
     const auto& nodes = g.nodes();
