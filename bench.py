@@ -190,11 +190,13 @@ def _workload(args):
 
 
 def _cpu_baseline(job_windows, n_sample, match, mismatch, gap):
+    """The CPU oracle on the first n_sample windows with every host thread:
+    (windows, seconds, DP cells, edge-cells, threads, [(consensus, polished)])."""
     import oracle
     blob = oracle.windows_blob(job_windows[:n_sample])
     threads = os.cpu_count() or 1
-    n, sec, cells = oracle.consensus_blob(blob, n_sample, threads, match, mismatch, gap, True)
-    return n, sec, cells, threads
+    n, sec, cells, ecells, res = oracle.consensus_blob_out(blob, n_sample, threads, match, mismatch, gap, True)
+    return n, sec, cells, ecells, threads, res
 
 
 def _serving_jobs(args):
@@ -655,11 +657,18 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = [job.window(i) for i in range(min(args.cpu_sample, n_win))]
-        n, sec, ccells, threads = _cpu_baseline(sample, len(sample), m, x, g)
+        n, sec, ccells, ecells, threads, cpu_res = _cpu_baseline(sample, len(sample), m, x, g)
         out["cpu_baseline"] = {"value": n / sec, "unit": "windows/s", "cores": threads, "kind": "port",
                                "gcups": ccells / sec / 1e9,
                                "sample": "first %d of %d windows, one pass (CPU oracle restatement of racon's "
                                          "algorithm; reference racon does not build here)" % (n, n_win)}
+        # parity on the timed workload: the oracle's consensus of the sampled
+        # windows against the device's from the timed steps
+        mism = sum(1 for a, b in zip(cpu_res, reference_out[:n]) if a != b)
+        out["parity"] = {"windows_checked": n, "mismatches": mism,
+                         "against": "CPU oracle, window by window (consensus bytes and polished flag)"}
+        # the sample's work counted by the oracle, scaled to the step by DP cells
+        out["compute"]["sample_edge_cells_per_cell"] = ecells / max(1, ccells)
     ctx.close()
     job.close()
     if world == 1 and args.serving_jobs > 0:

@@ -407,9 +407,10 @@ void rb_server_destroy(rb_server* server);
  *
  * query, target and distance are DEVICE pointers; the kernel runs one warp on
  * `stream` (a cudaStream_t, NULL = legacy default stream) and the call returns
- * without waiting for it. The current device's first call does one-time set-up
- * (loads the kernel, looks up the array's address) and should come before any
- * stream capture. All calls on a device share the array: it keeps the last
+ * without waiting for it. The current device's first call loads the kernel's
+ * module and should come before any stream capture; every call looks up the
+ * array's device address again (no allocation), so a call after a
+ * cudaDeviceReset uses the array of the new context. All calls on a device share the array: it keeps the last
  * call's contents and nothing in it needs to start at zero, but calls whose
  * kernels can overlap (different streams without ordering) race on it and
  * give wrong results, so order them on one stream. `err` (optional, capacity

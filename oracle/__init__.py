@@ -54,6 +54,11 @@ def load():
     lib.oracle_consensus_blob.restype = c.c_int64
     lib.oracle_consensus_blob.argtypes = [c.c_char_p, c.c_uint64, c.c_int64, c.c_uint32, c.c_int, c.c_int, c.c_int,
                                           c.c_int, c.POINTER(c.c_double), c.POINTER(c.c_uint64)]
+    lib.oracle_consensus_blob_out.restype = c.c_int64
+    lib.oracle_consensus_blob_out.argtypes = [c.c_char_p, c.c_uint64, c.c_int64, c.c_uint32, c.c_int, c.c_int,
+                                              c.c_int, c.c_int, c.POINTER(c.c_double), c.POINTER(c.c_uint64),
+                                              c.POINTER(c.c_uint64), c.c_char_p, c.c_uint64,
+                                              c.POINTER(c.c_uint64), c.POINTER(c.c_uint8)]
     _lib = lib
     return lib
 
@@ -239,3 +244,27 @@ def consensus_blob(blob, max_windows, threads, match, mismatch, gap, trim=True):
     if n < 0:
         raise RuntimeError("bad window blob")
     return n, sec.value, cells.value
+
+
+def consensus_blob_out(blob, max_windows, threads, match, mismatch, gap, trim=True, out_cap=None):
+    """As consensus_blob, and also the results: (windows done, seconds, DP
+    cells, edge-cells, [(consensus, polished)] per window). Edge-cells count
+    the DP work as sum |layer| x sum_v (1 + indeg v) over every alignment."""
+    lib = load()
+    (nw,) = struct.unpack_from("<Q", blob, 0)
+    n = min(nw, max_windows)
+    cap = out_cap or 4 * len(blob) + 1024
+    out = ctypes.create_string_buffer(cap)
+    offs = (ctypes.c_uint64 * (n + 1))()
+    pol = (ctypes.c_uint8 * max(1, n))()
+    sec = ctypes.c_double()
+    cells = ctypes.c_uint64()
+    ecells = ctypes.c_uint64()
+    r = lib.oracle_consensus_blob_out(blob, len(blob), max_windows, threads, match, mismatch, gap, int(trim),
+                                      ctypes.byref(sec), ctypes.byref(cells), ctypes.byref(ecells), out, cap,
+                                      offs, pol)
+    if r < 0:
+        raise RuntimeError("bad window blob or output too small")
+    raw = out.raw
+    res = [(raw[offs[i]:offs[i + 1]].decode(), bool(pol[i])) for i in range(r)]
+    return r, sec.value, cells.value, ecells.value, res

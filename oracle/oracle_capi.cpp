@@ -257,9 +257,16 @@ extern "C" {
 // oracle_dump_windows layout, on `threads` host threads. Returns the number of
 // windows done; *seconds = wall time of the consensus loop, *cells = DP cells.
 // Used as the CPU baseline (the oracle, not reference racon).
-int64_t oracle_consensus_blob(const char* blob, uint64_t nbytes, int64_t max_windows, uint32_t threads,
-                              int match, int mismatch, int gap, int trim, double* seconds,
-                              uint64_t* cells) {
+// Window consensus of up to max_windows windows of a blob in the
+// oracle_dump_windows layout on `threads` threads. When `out` is given, the
+// consensus of window i goes to out[offsets[i], offsets[i + 1]) (offsets has
+// room for n + 1 entries, out for out_cap bytes) and polished[i] is its
+// generate_consensus result; edge_cells (optional) gets the DP work counted
+// as sum |layer| x sum_v (1 + indeg v).
+int64_t oracle_consensus_blob_out(const char* blob, uint64_t nbytes, int64_t max_windows, uint32_t threads,
+                                  int match, int mismatch, int gap, int trim, double* seconds,
+                                  uint64_t* cells, uint64_t* edge_cells, char* out, uint64_t out_cap,
+                                  uint64_t* offsets, uint8_t* polished) {
     uint64_t off = 0;
     auto get = [&](void* dst, size_t n) {
         if (off + n > nbytes) return false;
@@ -297,26 +304,50 @@ int64_t oracle_consensus_blob(const char* blob, uint64_t nbytes, int64_t max_win
         wins.push_back(std::move(w));
         tgs.push_back(t);
     }
-    std::vector<uint64_t> c(wins.size(), 0);
+    std::vector<uint64_t> c(wins.size(), 0), ec(wins.size(), 0);
+    std::vector<std::string> cons(out ? wins.size() : 0);
+    std::vector<uint8_t> pol(wins.size(), 0);
     std::atomic<size_t> next(0);
     const auto t0 = std::chrono::steady_clock::now();
     std::vector<std::thread> pool;
     for (uint32_t k = 0; k < std::max<uint32_t>(1, threads); ++k) {
         pool.emplace_back([&]() {
             for (size_t i = next++; i < wins.size(); i = next++) {
-                std::string cons;
+                std::string cs;
                 WindowStats st;
-                window_consensus(wins[i], tgs[i] != 0, trim != 0, match, mismatch, gap, cons, &st);
+                pol[i] = window_consensus(wins[i], tgs[i] != 0, trim != 0, match, mismatch, gap, cs, &st);
                 c[i] = st.cells;
+                ec[i] = st.edge_cells;
+                if (out) cons[i].swap(cs);
             }
         });
     }
     for (auto& th : pool) th.join();
     *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    uint64_t total = 0;
+    uint64_t total = 0, etotal = 0;
     for (auto x : c) total += x;
+    for (auto x : ec) etotal += x;
     *cells = total;
+    if (edge_cells) *edge_cells = etotal;
+    if (out) {
+        uint64_t o = 0;
+        for (size_t i = 0; i < wins.size(); ++i) {
+            offsets[i] = o;
+            if (o + cons[i].size() > out_cap) return -2;
+            memcpy(out + o, cons[i].data(), cons[i].size());
+            o += cons[i].size();
+            polished[i] = pol[i];
+        }
+        offsets[wins.size()] = o;
+    }
     return int64_t(wins.size());
+}
+
+int64_t oracle_consensus_blob(const char* blob, uint64_t nbytes, int64_t max_windows, uint32_t threads,
+                              int match, int mismatch, int gap, int trim, double* seconds,
+                              uint64_t* cells) {
+    return oracle_consensus_blob_out(blob, nbytes, max_windows, threads, match, mismatch, gap, trim, seconds,
+                                     cells, nullptr, nullptr, 0, nullptr, nullptr);
 }
 
 }  // extern "C"

@@ -52,6 +52,7 @@ struct Request {
     double stage[4] = {0, 0, 0, 0};
     uint32_t worker = 0;
     bool done = false;
+    bool claimed = false;  // a thread is waiting on (or has taken) this ticket
     int status = RB_OK;
     std::string fasta, error;
 };
@@ -80,6 +81,7 @@ struct rb_server {
     uint64_t next_ticket = 1;
     uint64_t inflight_bytes = 0;
     uint32_t inflight = 0;
+    bool closing = false;  // rb_server_destroy has begun: submissions are refused
     bool stop = false;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
 
@@ -193,7 +195,7 @@ int rb_server_submit(rb_server* s, const rb_server_job* job, uint64_t* ticket) {
     r->footprint = s->estimate(*r);
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        if (s->stop) {
+        if (s->closing || s->stop) {
             t_server_error = "rb_server_submit: server is stopping";
             return RB_ERR_ARG;
         }
@@ -222,8 +224,13 @@ int rb_server_wait(rb_server* s, uint64_t ticket, char** fasta, rb_server_times*
             return RB_ERR_ARG;
         }
         r = it->second;
+        if (r->claimed) {
+            t_server_error = "rb_server_wait: ticket already waited for";
+            return RB_ERR_ARG;
+        }
+        r->claimed = true;
         s->cv_done.wait(lk, [&] { return r->done; });
-        s->jobs.erase(it);
+        s->jobs.erase(ticket);
     }
     if (times) {
         times->submitted = r->t_submit;
@@ -262,7 +269,9 @@ void rb_server_destroy(rb_server* s) {
     if (!s) return;
     {
         std::unique_lock<std::mutex> lk(s->mu);
-        // cancel what has not started; let the jobs in flight finish
+        // refuse new submissions, cancel what has not started, let the jobs
+        // in flight finish
+        s->closing = true;
         for (auto& r : s->queue) {
             r->status = RB_ERR_ARG;
             r->error = "rb_server: job cancelled (server destroyed)";

@@ -1580,8 +1580,6 @@ void NwEngine::fetch(rb_aln_result* out) {
 namespace {
 
 constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
 
 int noalloc_fail(char* err, uint32_t cap, int code, const char* fmt, ...) {
     if (err && cap) {
@@ -1611,28 +1609,16 @@ extern "C" int rb_nw_distance_noalloc(const char* query, uint32_t query_length, 
     if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
         return noalloc_fail(err, err_capacity, RB_ERR_CUDA, "rb_nw_distance_noalloc: no usable current device (CUDA error %d, device %d)",
                             int(e), dev);
+    // The scratch array's device address, looked up on every call: host code
+    // cannot take the address of a __device__ variable directly, and after a
+    // cudaDeviceReset (a new primary context) the module is loaded again and
+    // the array can move, so a cached address could be stale. The lookup
+    // allocates nothing. The device's first call also loads the module.
     void* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            // One-time set-up on this device: load the kernel and look up the
-            // device address of the scratch array. Host code cannot take the
-            // address of a __device__ variable directly.
-            cudaFuncAttributes fa;
-            e = cudaFuncGetAttributes(&fa, rb::nw_distance_noalloc_kernel);
-            if (e != cudaSuccess)
-                return noalloc_fail(err, err_capacity, RB_ERR_CUDA,
-                                    "rb_nw_distance_noalloc: kernel load failed: %s", cudaGetErrorString(e));
-            void* ptr = nullptr;
-            e = cudaGetSymbolAddress(&ptr, rb::g_noalloc_scratch);
-            if (e != cudaSuccess || !ptr)
-                return noalloc_fail(err, err_capacity, RB_ERR_CUDA,
-                                    "rb_nw_distance_noalloc: scratch address lookup failed: %s",
-                                    cudaGetErrorString(e));
-            g_noalloc_ptr[dev] = ptr;
-        }
-        scratch = g_noalloc_ptr[dev];
-    }
+    e = cudaGetSymbolAddress(&scratch, rb::g_noalloc_scratch);
+    if (e != cudaSuccess || !scratch)
+        return noalloc_fail(err, err_capacity, RB_ERR_CUDA, "rb_nw_distance_noalloc: scratch address lookup failed: %s",
+                            cudaGetErrorString(e));
     rb::nw_distance_noalloc_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(
         query, query_length, target, target_length, distance, static_cast<uint8_t*>(scratch));
     e = cudaGetLastError();

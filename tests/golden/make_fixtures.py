@@ -59,4 +59,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/test/data")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <racon checkout>/test/data")
+    main(sys.argv[1])

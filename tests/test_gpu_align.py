@@ -101,6 +101,36 @@ def test_lambda_ava_overlaps_sample(ctx, oracle_lib):
     _check(ctx, oracle_lib, pairs, 500)
 
 
+def _check_parallel(ctx, oracle_lib, pairs, window_length):
+    """_check with the oracle's alignments computed on every host thread."""
+    import concurrent.futures
+    import os
+    got = ctx.align(pairs, want_cigar=True)
+    with concurrent.futures.ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        want = list(ex.map(lambda p: oracle_lib.nw_cigar(p["query"], p["target"]), pairs))
+    bad = 0
+    for p, g, (d, cig) in zip(pairs, got, want):
+        exp_bp = oracle_lib.breakpoints(cig, p["q_offset"], p["q_offset"] + len(p["query"]),
+                                        p["q_offset"] + len(p["query"]), p["t_begin"],
+                                        p["t_begin"] + len(p["target"]), 0, window_length)
+        if (g["edit_distance"], g["cigar"], g["breakpoints"]) != (d, cig, exp_bp):
+            bad += 1
+    assert bad == 0, "%d of %d pairs differ" % (bad, len(pairs))
+
+
+def test_config2_long_pairs(ctx, oracle_lib):
+    # the overlap-alignment batch's longest spans: 30-50 kb targets, query at
+    # 7% sub + 4% ins + 4% del (Hirschberg splits many levels deep)
+    from racon_b200 import synthetic
+    _check_parallel(ctx, oracle_lib, synthetic.pairs(48, 30_000, 50_000, seed=21), 500)
+
+
+def test_config2_batch_sample(ctx, oracle_lib):
+    # 1000 pairs with the batch's full span range, 1-50 kb
+    from racon_b200 import synthetic
+    _check_parallel(ctx, oracle_lib, synthetic.pairs(1000, 1_000, 50_000, seed=22), 500)
+
+
 def test_stage_run_fetch_matches_batch(ctx, oracle_lib):
     pairs = _random_pairs(5, 50, 100, 2000, 0.12)
     a = ctx.align(pairs, want_cigar=True)

@@ -15,20 +15,56 @@ pytestmark = pytest.mark.gpu
 GOLDENS = json.load(open(os.path.join(GOLDEN, "goldens.json")))
 
 
+_DEVICE = {}
+
+
+def _device_fasta(native_lib, g):
+    if g["name"] not in _DEVICE:
+        kw = dict(fragment=bool(g["fragment"]), window_length=g["window_length"], match=g["match"],
+                  mismatch=g["mismatch"], gap=g["gap"], drop_unpolished=bool(g["drop_unpolished"]))
+        paths = (lambda_path(g["reads"]), lambda_path(g["overlaps"]), lambda_path(g["targets"]))
+        _DEVICE[g["name"]] = native_lib.polish_files(*paths, **kw)
+    return _DEVICE[g["name"]]
+
+
 @pytest.mark.parametrize("g", GOLDENS, ids=[g["name"] for g in GOLDENS])
 def test_pipeline_matches_oracle(native_lib, oracle_lib, g):
     kw = dict(fragment=bool(g["fragment"]), window_length=g["window_length"], match=g["match"],
               mismatch=g["mismatch"], gap=g["gap"], drop_unpolished=bool(g["drop_unpolished"]))
     paths = (lambda_path(g["reads"]), lambda_path(g["overlaps"]), lambda_path(g["targets"]))
-    dev = native_lib.polish_files(*paths, **kw)
     ref, _, _ = oracle_lib.polish(*paths, threads=8, **kw)
-    assert dev == ref
+    assert _device_fasta(native_lib, g) == ref
+
+
+# The one golden the whole stack misses by a single base in 1.66 Mb: the
+# device output equals the oracle's, which gives 1663983 where racon's test
+# expects 1663982 (a tie that the absent third-party consensus code breaks
+# differently). Marked strict, so a fix shows up as XPASS.
+KNOWN_OFF = {"FragmentCorrectionWithoutQualitiesFull"}
+
+
+def _golden_params():
+    out = []
+    for g in GOLDENS:
+        marks = [pytest.mark.xfail(strict=True, reason="one base off racon's golden total length")] \
+            if g["name"] in KNOWN_OFF else []
+        out.append(pytest.param(g, id=g["name"], marks=marks))
+    return out
+
+
+@pytest.mark.parametrize("g", _golden_params())
+def test_pipeline_racon_golden(native_lib, oracle_lib, g):
+    """racon's own golden numbers (test/racon_test.cpp:88-290) on the device
+    path's FASTA: the edit distance to the reference genome, or the sequence
+    count and total length."""
+    dev = _device_fasta(native_lib, g)
     exp = g["expected"]
     lines = dev.split("\n")
     recs = [lines[i + 1] for i in range(0, len(lines) - 1, 2)]
     if "edit_distance" in exp:
         with gzip.open(lambda_path("sample_reference.fasta.gz"), "rt") as fh:
             truth = "".join(l.strip() for l in fh if not l.startswith(">"))
+        assert len(recs) == 1
         assert oracle_lib.nw_distance(revcomp(recs[0]), truth) == exp["edit_distance"]
     else:
-        assert len(recs) == exp["sequences"]
+        assert {"sequences": len(recs), "total_length": sum(len(r) for r in recs)} == exp
