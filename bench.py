@@ -58,6 +58,7 @@ def _args():
     p.add_argument("--scale", type=float, default=1.0, help="genome scale (1.0 = the named workload)")
     p.add_argument("--cpu-sample", type=int, default=400, help="windows in the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true", help="keep the default launch choices")
     p.add_argument("--data-dir", default=None)
     p.add_argument("--serving-jobs", type=int, default=12, help="config-4 jobs in the serving measurement "
                    "(0 = skip it)")
@@ -318,6 +319,7 @@ def run_align(args, local, world, rank):
     ctx = racon_b200.Context(local)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     ctx.align_stage(pairs, want_cigar=True)
+    tuning = None if args.no_autotune else ctx.autotune(consensus=False, alignment=True)
     for _ in range(args.warmup):
         ctx.align_run()
     ref = ctx.align_fetch()
@@ -384,7 +386,7 @@ def run_align(args, local, world, rank):
            "compute": {"bound": "int32 issue", "achieved_tops": achieved_tops, "peak_tops": int_peak_tops,
                        "frac": achieved_tops / int_peak_tops, "band_words": words,
                        "note": "minimal band of the final distance x 34 int32 ops per 64-row word"},
-           "clocks": clk}
+           "clocks": clk, "tuning": tuning}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = pairs[:256]
         threads = os.cpu_count() or 1
@@ -519,13 +521,18 @@ def main():
 
     # ---- device-resident throughput ----
     ctx.poa_stage_job(job)
+    tuning = None
+    if not args.no_autotune:
+        # the device's launch choices measured on this job's windows (every
+        # candidate gives the same consensus; checked inside rb_autotune)
+        tuning = ctx.autotune(consensus=True)
     for _ in range(args.warmup):
         ctx.poa_run()
     reference_out = ctx.poa_fetch()
     clocks = Clocks(local)
     barrier()
     clocks.start()
-    kms, launches, cells = [], 0, 0
+    kms, launches, cells, ecells = [], 0, 0, 0
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -534,6 +541,7 @@ def main():
         kms.append(st.kernel_ms)
         launches += st.launches
         cells += st.cells
+        ecells += st.edge_cells
     barrier()
     clk = clocks.stop()
     assert ctx.poa_fetch() == reference_out, "device results changed between steps"
@@ -610,8 +618,10 @@ def main():
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     int_peak_tops = sm_count * 128 * sm_mhz * 1e6 / 1e12
-    # ~6 int32 ops per DP cell edge (two add-max pairs, scan step, decision test)
-    achieved_tops = cells * 6 / dev_s / 1e12
+    # counted work: edge-cells (|layer| x sum over the aligned rows of
+    # 1 + predecessors, counted by the kernel) x 3 int32 ops (add, max,
+    # compare-select per max-plus term)
+    achieved_tops = ecells * 3 / dev_s / 1e12
     out = {
         "metric": "POA windows/s", "value": value, "unit": "windows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * dev_s_max / args.steps, "higher_is_better": True,
@@ -646,8 +656,13 @@ def main():
                              "bound, see compute"},
         "compute": {"bound": "int32 issue", "achieved_tops": achieved_tops, "peak_tops": int_peak_tops,
                     "frac": achieved_tops / int_peak_tops, "gcups": gcups,
-                    "note": "peak = SMs x 128 int32 lanes x median SM clock under load; ~6 int ops per cell"},
+                    "edge_cells_per_step": ecells // max(1, args.steps),
+                    "edge_cells_per_cell": ecells / max(1, cells),
+                    "note": "achieved = edge-cells counted on the device (|layer| x sum_v (1 + in-degree v) over "
+                            "the aligned graph) x 3 int32 ops / device time; peak = SMs x 128 int32 lanes x median "
+                            "SM clock under load"},
         "clocks": clk,
+        "tuning": tuning,
         "stages_s": {"load": job.stage_seconds[0], "align": job.stage_seconds[1], "layers": job.stage_seconds[2],
                      "note": "align = sequence table to the device, overlap alignment and (PAF/MHAP) the "
                              "device layer assembly; layers = the host's window records"},
@@ -657,7 +672,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = [job.window(i) for i in range(min(args.cpu_sample, n_win))]
-        n, sec, ccells, ecells, threads, cpu_res = _cpu_baseline(sample, len(sample), m, x, g)
+        n, sec, ccells, cpu_ecells, threads, cpu_res = _cpu_baseline(sample, len(sample), m, x, g)
         out["cpu_baseline"] = {"value": n / sec, "unit": "windows/s", "cores": threads, "kind": "port",
                                "gcups": ccells / sec / 1e9,
                                "sample": "first %d of %d windows, one pass (CPU oracle restatement of racon's "
@@ -667,8 +682,9 @@ def main():
         mism = sum(1 for a, b in zip(cpu_res, reference_out[:n]) if a != b)
         out["parity"] = {"windows_checked": n, "mismatches": mism,
                          "against": "CPU oracle, window by window (consensus bytes and polished flag)"}
-        # the sample's work counted by the oracle, scaled to the step by DP cells
-        out["compute"]["sample_edge_cells_per_cell"] = ecells / max(1, ccells)
+        # the same work unit counted by the oracle on its sample, beside the
+        # device's count over the whole step
+        out["compute"]["oracle_sample_edge_cells_per_cell"] = cpu_ecells / max(1, ccells)
     ctx.close()
     job.close()
     if world == 1 and args.serving_jobs > 0:

@@ -270,6 +270,36 @@ int rb_set_yield(rb_ctx* ctx, uint32_t consensus_windows, uint32_t alignment_ite
 int rb_set_sm_share(rb_ctx* ctx, uint32_t percent);
 int rb_set_priority(rb_ctx* ctx, int high);
 
+/* ---------------------------------------------------------------------
+ * Autotuner (no counterpart in the reference: racon's CUDA plug-in sizes its
+ * batches from fixed constants, src/cuda/cudapolisher.cpp:158-180 and
+ * BatchConfig(1023, 200, 256, band) at src/cuda/cudabatch.cpp:56-59).
+ * ------------------------------------------------------------------- */
+
+/* Launch choices of one device, shared by every context on it. None of them
+ * changes a result. */
+typedef struct rb_tuning {
+    uint32_t consensus_ctas_per_sm;   /* resident consensus CTAs per SM, 1..3 (4 windows each): windows in flight */
+    uint32_t consensus_order;         /* queue order: 0 heaviest window first; 1 size buckets interleaved
+                                       * (heaviest, lightest, next heaviest, ...) */
+    uint32_t alignment_warps_per_sm;  /* resident alignment warps per SM (one pair or split task each): 4..32 */
+    uint32_t tuned;                   /* bit 0: consensus choices measured, bit 1: alignment choices measured */
+    double consensus_ms;              /* kernel time of the chosen consensus setting on the tuning batch */
+    double alignment_ms;              /* kernel time of the chosen alignment setting on the tuning batch */
+} rb_tuning;
+
+/* Measures the candidate launch choices on the batch staged in ctx and keeps
+ * the fastest for the device: what & 1 sweeps consensus CTAs per SM x queue
+ * order over the staged windows (rb_poa_stage*), what & 2 the resident
+ * alignment warps over the staged pairs (rb_align_stage*). Every candidate
+ * run must give identical results (checked; RB_ERR_DEVICE otherwise). The
+ * staged batch and its results stay as after one run. */
+int rb_autotune(rb_ctx* ctx, int what);
+/* The device's current choices (defaults until tuned or set). */
+int rb_tuning_get(int device, rb_tuning* out);
+/* Pins the device's choices (values are clamped to their ranges). */
+int rb_tuning_set(int device, const rb_tuning* in);
+
 /* Counters of the last run/batch call of each kind. */
 typedef struct rb_stats {
     double kernel_ms;        /* device time of the compute kernels (CUDA events) */
@@ -280,6 +310,8 @@ typedef struct rb_stats {
     uint64_t items;          /* windows or pairs processed */
     uint32_t max_nodes;      /* POA: largest graph seen */
     double top_kernel_ms;    /* device time of the dominant kernel */
+    uint64_t edge_cells;     /* POA: sum over alignments of |layer| x sum_v (1 + in-degree of v)
+                              * over the aligned (sub)graph: the DP's max-plus terms */
 } rb_stats;
 int rb_poa_stats(const rb_ctx* ctx, rb_stats* out);
 int rb_align_stats(const rb_ctx* ctx, rb_stats* out);
@@ -343,9 +375,19 @@ void rb_free(void* p);
  * job and concurrent jobs' kernels overlap on the GPU. hbm_budget: device
  * bytes the jobs in flight may take by estimate; a queued job is admitted,
  * first in first out, when a worker is idle and its estimated footprint fits
- * beside the jobs in flight (a job alone is always admitted). Each worker's
- * window-consensus scratch is also capped at hbm_budget / workers. 0 selects
- * 4 workers and 75% of the device memory. */
+ * beside the jobs in flight (a job alone is always admitted). 0 selects
+ * 4 workers and 75% of the device memory.
+ *
+ * Window consensus is continuously batched: one persistent consensus kernel
+ * per server takes windows of every job in flight from a shared device work
+ * queue, so a job admitted while others run starts on the first free warps
+ * instead of waiting for their launches to drain. Jobs of at most
+ * priority_windows windows (0: a quarter of the kernel's resident windows)
+ * go to a high-priority queue that the kernel drains first.
+ * consensus_ctas_per_sm (0 or more than 2: 2) sizes that kernel; the rest of each
+ * SM stays free for the alignment and layer kernels of newly admitted jobs.
+ * shared_consensus = 0 turns the shared kernel off (each job then launches
+ * its own consensus kernel, with its scratch capped at hbm_budget / workers). */
 typedef struct rb_server_params {
     int device;
     uint32_t workers;
@@ -354,6 +396,9 @@ typedef struct rb_server_params {
     int8_t mismatch;
     int8_t gap;
     uint32_t window_length;
+    int shared_consensus;
+    uint32_t consensus_ctas_per_sm;
+    uint32_t priority_windows;
 } rb_server_params;
 
 /* One job: racon's inputs and per-job flags (-f, -q, -e, --no-trimming, -u). */

@@ -91,7 +91,8 @@ class _PoaResult(ctypes.Structure):
 class _ServerParams(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
                 ("match", ctypes.c_int8), ("mismatch", ctypes.c_int8), ("gap", ctypes.c_int8),
-                ("window_length", ctypes.c_uint32)]
+                ("window_length", ctypes.c_uint32), ("shared_consensus", ctypes.c_int),
+                ("consensus_ctas_per_sm", ctypes.c_uint32), ("priority_windows", ctypes.c_uint32)]
 
 
 class _ServerJob(ctypes.Structure):
@@ -106,11 +107,21 @@ class ServerTimes(ctypes.Structure):
                 ("stage_seconds", ctypes.c_double * 4), ("footprint", ctypes.c_uint64), ("worker", ctypes.c_uint32)]
 
 
+class Tuning(ctypes.Structure):
+    """rb_tuning: a device's launch choices (none changes a result)."""
+    _fields_ = [("consensus_ctas_per_sm", ctypes.c_uint32), ("consensus_order", ctypes.c_uint32),
+                ("alignment_warps_per_sm", ctypes.c_uint32), ("tuned", ctypes.c_uint32),
+                ("consensus_ms", ctypes.c_double), ("alignment_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("launches", ctypes.c_uint64),
                 ("cells", ctypes.c_uint64), ("items", ctypes.c_uint64), ("max_nodes", ctypes.c_uint32),
-                ("top_kernel_ms", ctypes.c_double)]
+                ("top_kernel_ms", ctypes.c_double), ("edge_cells", ctypes.c_uint64)]
 
 
 _lib = None
@@ -157,6 +168,9 @@ def load():
     lib.rb_set_yield.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32]
     lib.rb_set_priority.argtypes = [vp, ctypes.c_int]
     lib.rb_set_sm_share.argtypes = [vp, ctypes.c_uint32]
+    lib.rb_autotune.argtypes = [vp, ctypes.c_int]
+    lib.rb_tuning_get.argtypes = [ctypes.c_int, ctypes.POINTER(Tuning)]
+    lib.rb_tuning_set.argtypes = [ctypes.c_int, ctypes.POINTER(Tuning)]
     lib.rb_sequence_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.rb_job_layer_input.argtypes = [vp, ctypes.POINTER(ctypes.POINTER(_Sequence)),
                                        ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
@@ -209,6 +223,7 @@ class Context:
         self.ptr = self.lib.rb_create(device, ctypes.byref(p))
         if not self.ptr:
             raise RaconB200Error(5, self.lib.rb_create_error().decode())
+        self.device = device
         self.window_length = window_length
         self._keep = None
 
@@ -471,6 +486,12 @@ class Context:
         """Percent of the SMs the persistent kernels fill; rb_set_sm_share."""
         self._check(self.lib.rb_set_sm_share(self.ptr, percent))
 
+    def autotune(self, consensus=True, alignment=False):
+        """rb_autotune on the staged batch(es): keeps the fastest launch
+        choices for the device; returns them as a dict."""
+        self._check(self.lib.rb_autotune(self.ptr, (1 if consensus else 0) | (2 if alignment else 0)))
+        return tuning_get(self.device)
+
     def set_priority(self, high):
         """High- or normal-priority stream for this context; rb_set_priority."""
         self._check(self.lib.rb_set_priority(self.ptr, int(high)))
@@ -602,14 +623,20 @@ class Server:
     workers jobs run at once, each on a long-lived device context of its own;
     queued jobs are admitted first in first out when a worker is idle and the
     job's estimated device footprint fits in hbm_budget beside the jobs in
-    flight. submit() returns a ticket; wait(ticket) returns (fasta, times)."""
+    flight. With shared_consensus (the default) one persistent consensus
+    kernel takes the windows of every job in flight from a shared device
+    queue (continuous batching); jobs of at most priority_windows windows go
+    first. submit() returns a ticket; wait(ticket) returns (fasta, times)."""
 
-    def __init__(self, device=0, workers=4, hbm_budget=0, match=3, mismatch=-5, gap=-4, window_length=500):
+    def __init__(self, device=0, workers=4, hbm_budget=0, match=3, mismatch=-5, gap=-4, window_length=500,
+                 shared_consensus=True, consensus_ctas_per_sm=0, priority_windows=0):
         self.lib = load()
-        p = _ServerParams(device, workers, hbm_budget, match, mismatch, gap, window_length)
+        p = _ServerParams(device, workers, hbm_budget, match, mismatch, gap, window_length, int(shared_consensus),
+                          consensus_ctas_per_sm, priority_windows)
         self.ptr = self.lib.rb_server_create(ctypes.byref(p))
         if not self.ptr:
-            raise RaconB200Error(5, self.lib.rb_create_error().decode())
+            msg = self.lib.rb_server_error().decode() or self.lib.rb_create_error().decode()
+            raise RaconB200Error(5, msg)
 
     def submit(self, sequences, overlaps, targets, fragment=False, quality_threshold=10.0, error_threshold=0.3,
                trim=True, drop_unpolished=True):
@@ -656,3 +683,22 @@ class Server:
         except Exception:
             pass
 
+
+def tuning_get(device=0):
+    """The device's launch choices (rb_tuning_get) as a dict."""
+    t = Tuning()
+    rc = load().rb_tuning_get(device, ctypes.byref(t))
+    if rc != RB_OK:
+        raise RaconB200Error(rc, "rb_tuning_get failed")
+    return t.as_dict()
+
+
+def tuning_set(device=0, **values):
+    """Pins some of the device's launch choices (rb_tuning_set); the others
+    keep their current values."""
+    cur = tuning_get(device)
+    cur.update(values)
+    t = Tuning(**{k: cur[k] for k, _ in Tuning._fields_})
+    rc = load().rb_tuning_set(device, ctypes.byref(t))
+    if rc != RB_OK:
+        raise RaconB200Error(rc, "rb_tuning_set failed")

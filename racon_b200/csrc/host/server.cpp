@@ -72,6 +72,7 @@ struct rb_server {
     rb_server_params params{};
     int sm_count = 148;
     uint64_t poa_cap = 0;
+    std::unique_ptr<rb::PoaService> svc;  // shared consensus kernel (continuous batching)
     std::vector<rb_ctx*> ctxs;
     std::vector<std::thread> threads;
     std::mutex mu;
@@ -90,14 +91,15 @@ struct rb_server {
     }
 
     // Device bytes a job is expected to hold: its inputs on the device, the
-    // alignment scratch and one consensus slot per resident window.
+    // alignment scratch and (without the shared consensus kernel, whose
+    // scratch is allocated once) one consensus slot per resident window.
     uint64_t estimate(const Request& r) const {
         const uint64_t reads = file_bytes(r.sp), targets = file_bytes(r.tp);
         const uint64_t w = std::max<uint32_t>(1, params.window_length);
         const uint64_t windows = targets / w + 1;
         const uint64_t resident = std::min<uint64_t>(windows, uint64_t(sm_count) * 12);
         const uint64_t slot = rb::PoaEngine::slot_bytes_for(uint32_t(std::min<uint64_t>(3 * w, 65535)));
-        const uint64_t poa = std::min<uint64_t>(resident * slot, poa_cap);
+        const uint64_t poa = svc ? 0 : std::min<uint64_t>(resident * slot, poa_cap);
         const uint64_t align = std::min<uint64_t>(uint64_t(4) << 30, (reads + targets) * 8 + (uint64_t(256) << 20));
         return poa + align + 3 * (reads + targets);
     }
@@ -175,6 +177,25 @@ rb_server* rb_server_create(const rb_server_params* params) {
     }
     s->poa_cap = s->params.hbm_budget / s->params.workers;
     for (rb_ctx* c : s->ctxs) rb::ctx_set_poa_budget(c, s->poa_cap);
+    if (s->params.shared_consensus) {
+        // the shared kernel's scratch comes out of the budget once; each
+        // worker keeps a small private budget for windows that outgrow it
+        const uint32_t cps = s->params.consensus_ctas_per_sm ? s->params.consensus_ctas_per_sm : 2;
+        try {
+            s->svc.reset(new rb::PoaService(params->device, params->match, params->mismatch, params->gap,
+                                            params->window_length, s->params.hbm_budget / 2, cps));
+        } catch (const rb::Error& e) {
+            for (rb_ctx* x : s->ctxs) rb_destroy(x);
+            t_server_error = e.msg;
+            return nullptr;
+        }
+        const uint32_t prio = s->params.priority_windows ? s->params.priority_windows : s->svc->slots() / 4;
+        s->params.priority_windows = prio;
+        for (rb_ctx* c : s->ctxs) {
+            rb::ctx_set_poa_budget(c, s->params.hbm_budget / 2 / s->params.workers);
+            rb::ctx_set_poa_service(c, s->svc.get(), prio);
+        }
+    }
     for (uint32_t i = 0; i < s->params.workers; ++i) s->threads.emplace_back([srv = s.get(), i] { srv->worker(i); });
     return s.release();
 }
@@ -286,6 +307,7 @@ void rb_server_destroy(rb_server* s) {
     s->cv_work.notify_all();
     for (auto& t : s->threads) t.join();
     for (rb_ctx* c : s->ctxs) rb_destroy(c);
+    s->svc.reset();
     delete s;
 }
 

@@ -1321,9 +1321,10 @@ void NwEngine::reserve_scratch(uint32_t max_m, uint32_t max_n) {
     const size_t nb = (size_t(max_m) + 63) / 64 + 1;
     const size_t ncols = size_t(max_n) + 64;
     scratch_stride_ = warp_scratch_bytes(ncols, nb);
-    // warps: enough to fill the context's share of the SMs (all by default),
-    // bounded by a scratch budget of 4 GiB
-    size_t warps = std::max<size_t>(kWarpsPerBlock, size_t(dev_.sm_count) * 16 * sm_share_pct_ / 100);
+    // warps: the device's tuned warps per SM on the context's share of the
+    // SMs (all by default), bounded by a scratch budget of 4 GiB
+    const size_t per_sm = tuning_get(dev_.device).alignment_warps_per_sm;
+    size_t warps = std::max<size_t>(kWarpsPerBlock, size_t(dev_.sm_count) * per_sm * sm_share_pct_ / 100);
     const size_t budget = size_t(4) << 30;
     while (warps > size_t(kWarpsPerBlock) && warps * scratch_stride_ > budget) warps /= 2;
     warps = (warps / kWarpsPerBlock) * kWarpsPerBlock;

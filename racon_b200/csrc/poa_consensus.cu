@@ -40,6 +40,24 @@
 #include "rb_internal.hpp"
 
 namespace rb {
+
+// One batch of windows in the shared queue (host-mapped record, written
+// before its items are published): the batch's device buffers, as PoaArgs
+// holds them for a private launch.
+struct PoaJobDev {
+    const uint8_t* in;
+    const PoaWinDev* wins;
+    const PoaLayerDev* layers;
+    char* out;
+    uint32_t* out_len;
+    uint8_t* flags;
+    unsigned long long* cells;  // [0] DP cells, [1] edge-cells (device)
+    uint32_t total;             // windows of the batch
+    int trim;
+    uint32_t generation;        // written to the finished flag when the batch is done
+    uint32_t pad;
+};
+
 namespace {
 
 // minus infinity that survives thousands of gap additions without overflow
@@ -71,7 +89,7 @@ struct PoaArgs {
     int match, mismatch, gap;
     int trim;
     unsigned int* counters;      // [0] window cursor, [1] status
-    unsigned long long* cells;   // DP cells computed
+    unsigned long long* cells;   // [0] DP cells computed, [1] edge-cells
     uint32_t per_warp_cap;       // windows a warp takes per launch (0: until the queue is empty)
 };
 
@@ -96,6 +114,7 @@ struct Graph {
     int *ord, *ord2, *my_rank, *shift, *nw_node, *nw_slot;
     int* H;
     uint8_t* dec;
+    int* lastH;   // per DP row (sinks): score of the last column
     // per-node in-edge and aligned-entry counts, owner node of each aligned
     // entry (for the compact lists built in shared memory)
     int *in_cnt, *al_cnt, *a_owner, *out_cnt;
@@ -180,6 +199,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
     take(S * 4, 23);       // stack
     take((N + 1) * L * 4, 31);  // H
     take(std::max(((N + 8) & ~size_t(7)) * L, (N + 1) * 256), 32);  // dec: bytes, or 32 uint2 per row
+    take((N + 1) * 4, 44);      // lastH: last-column score of each sink row
     // whole 2 MiB pages per slot, so that a slot's graph arrays share one page
     off = (off + (size_t(2) << 20) - 1) & ~((size_t(2) << 20) - 1);
     return off;
@@ -188,7 +208,7 @@ __host__ __device__ size_t walk_layout(int ncap, int ecap, int acap, int lcap, F
 __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
     uint8_t* base = a.scratch + size_t(slot) * a.slot_bytes;
     Graph g;
-    void* p[44];
+    void* p[45];
     walk_layout(a.ncap, a.ecap, a.acap, a.lcap, [&](int id, size_t off) { p[id] = base + off; });
     g.code = (uint8_t*)p[0];
     g.cov = (uint32_t*)p[1];
@@ -234,6 +254,7 @@ __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
     g.al_cnt = (int*)p[41];
     g.a_owner = (int*)p[42];
     g.out_cnt = (int*)p[43];
+    g.lastH = (int*)p[44];
     g.ncap = a.ncap;
     g.ecap = a.ecap;
     g.acap = a.acap;
@@ -248,6 +269,7 @@ __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
 // last-column value, that value, and how many sinks share it.
 struct EndCell {
     int row, value, ties;
+    int preds;  // predecessor links over the DP rows (edge-cells = |layer| x (rows + preds))
 };
 
 struct PoaShared {
@@ -892,11 +914,12 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
     for (int j = lane; j < nch * ch; j += 32) Hm[j] = j * gap;
     __syncwarp();
     const int lane_l = (L % ch) / S, k_l = L % S, ch_l = L / ch;
-    int best_v = kNegInf, best_r = INT_MAX, ties = 0;
+    int best_v = kNegInf, best_r = INT_MAX, ties = 0, npreds = 0;
     for (int i = 1; i <= ndp; ++i) {
         const int4 d = g.rowdesc[i - 1];
         const uint32_t cmask = desc_base(d.w) * 0x01010101u;
         const int np = desc_np(d.w);
+        npreds += np;
         const int cnt = np == 0 ? 1 : np;
         const bool is_sink = desc_sink(d.w);
         int carry_in = kNegInf;  // final H of the last column of the previous chunk
@@ -1002,6 +1025,7 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
 #pragma unroll
                 for (int k = 0; k < S; ++k)
                     if (k == k_l) val = hrow[k];
+                g.lastH[i] = val;
                 if (val > best_v) {
                     best_v = val;
                     best_r = i;
@@ -1016,7 +1040,7 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
     }
     // the owner lane of column L holds the end cell
     return EndCell{__shfl_sync(kFull, best_r, lane_l), __shfl_sync(kFull, best_v, lane_l),
-                   __shfl_sync(kFull, ties, lane_l)};
+                   __shfl_sync(kFull, ties, lane_l), npreds};
 }
 
 // last 512 bytes of each warp's ring hold the 32-row descriptor block
@@ -1068,7 +1092,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
 #pragma unroll
     for (int k = 0; k < S; ++k) Hm[j0 + k] = (j0 + k) * gap;
     const int lane_l = L / S, k_l = L % S;
-    int best_v = kNegInf, best_r = INT_MAX, ties = 0;
+    int best_v = kNegInf, best_r = INT_MAX, ties = 0, npreds = 0;
     int4* const dblk = ring + kRingDescOffset;
     const int4* const rowdesc = g.rowdesc;
     int4 pre = lane < ndp ? rowdesc[lane] : make_int4(0, 0, 0, 0);
@@ -1083,6 +1107,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         }
         const int4 d = dblk[bi];
         const int np = desc_np(d.w);
+        npreds += np;
         const bool is_sink = desc_sink(d.w);
         const uint32_t cmask = desc_base(d.w) * 0x01010101u;
         const int p0 = np > 3 ? d.y : d.x;
@@ -1188,6 +1213,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
 #pragma unroll
             for (int k = 0; k < S; ++k)
                 if (k == k_l) val = hv[k];
+            g.lastH[i] = val;
             if (val > best_v) {
                 best_v = val;
                 best_r = i;
@@ -1199,7 +1225,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
     }
     __syncwarp();
     return EndCell{__shfl_sync(kFull, best_r, lane_l), __shfl_sync(kFull, best_v, lane_l),
-                   __shfl_sync(kFull, ties, lane_l)};
+                   __shfl_sync(kFull, ties, lane_l), npreds};
 }
 
 // True when the layer's DP runs in dp_layer_fast (bit-plane decisions).
@@ -1914,6 +1940,7 @@ __device__ bool traceback_warp(const PoaArgs& a, const Graph& g, PoaShared& sh, 
                     w_node[o] = order[r - 1];
                     w_bits[o] = D2[bits_at(r, seg)];
                     w_bits[W + o] = seg > 0 ? D2[bits_at(r, seg - 1)] : make_uint2(0, 0);
+
                 }
             }
             __syncwarp();
@@ -2023,7 +2050,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         sh.fail = 0;
     }
     __syncwarp();
-    unsigned long long cells = 0;
+    unsigned long long cells = 0, edge_cells = 0;
 
     for (uint32_t li = 0; li < W.n_layers; ++li) {
         const PoaLayerDev Lr = a.layers[W.layer_base + li];
@@ -2177,6 +2204,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         }
         const EndCell ec = dp_dispatch(a, g, order, ndp, seq, L, lane, ring);
         cells += (unsigned long long)ndp * (unsigned long long)L;
+        edge_cells += (unsigned long long)(ndp + ec.preds) * (unsigned long long)L;
         int iend = ec.row;
         if (ec.ties > 1) {
             // several sinks share the best last-column value: spoa takes the
@@ -2188,7 +2216,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
             int low_id = INT_MAX, low_i = iend;
             bool grouped = false;
             for (int i = 1 + lane; i <= ndp; i += 32) {
-                if (!g.sink[i - 1] || g.H[i * g.lcap + L] != ec.value) continue;
+                if (!g.sink[i - 1] || g.lastH[i] != ec.value) continue;
                 const int v = order[i - 1];
                 grouped |= g.al_cnt[v] != 0;
                 if (v < low_id) {
@@ -2217,7 +2245,7 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
                 // the tied sink of lowest rank (ranks are distinct)
                 int best = INT_MAX, bi = iend;
                 for (int i = 1 + lane; i <= ndp; i += 32) {
-                    if (!g.sink[i - 1] || g.H[i * g.lcap + L] != ec.value) continue;
+                    if (!g.sink[i - 1] || g.lastH[i] != ec.value) continue;
                     const int rr = g.node_rank[order[i - 1]];
                     if (rr < best) {
                         best = rr;
@@ -2257,7 +2285,10 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
         }
         __syncwarp();
     }
-    if (lane == 0 && cells) atomicAdd(a.cells, cells);
+    if (lane == 0 && cells) {
+        atomicAdd(a.cells, cells);
+        atomicAdd(a.cells + 1, edge_cells);
+    }
     if (sh.fail) {
         if (lane == 0) {
             a.flags[wi] = uint8_t(sh.fail);
@@ -2353,6 +2384,126 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) poa_plain_kerne
     if (lane == 0) g = make_graph(a, blockIdx.x);
     __syncwarp();
     poa_window(a, g, sh, a.order[blockIdx.x], lane, ring_all);
+}
+
+// ---------------- shared queue (serving) ----------------
+
+// Loads with acquire semantics at system scope: the host publishes queue
+// items and job records in mapped host memory, then the tail.
+__device__ __forceinline__ unsigned long long ld_acquire_sys(const volatile unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned int ld_acquire_sys32(const volatile unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+struct PoaSvcArgs {
+    PoaArgs base;                                // scoring, capacities, scratch slots
+    const PoaJobDev* jobs;                       // mapped host: job records
+    const uint2* items[2];                       // mapped host rings: (job slot, window), [0] = high priority
+    const volatile unsigned long long* tail[2];  // mapped host: items published
+    unsigned long long* head[2];                 // device: items claimed
+    unsigned long long ring_mask;
+    unsigned int* done;                          // device: windows finished per job slot
+    volatile unsigned int* finished;             // mapped host: generation of the last finished batch per slot
+    const volatile unsigned int* stop;           // mapped host: leave now
+    unsigned long long idle_ns;                  // a warp leaves after this long without work
+};
+
+// Claims the next item, high-priority ring first: returns (job << 32) |
+// window, or ~0 after idle_ns without work or when stop is set (bounded: the
+// kernel always ends). Out of line with scalar arguments, so its registers
+// do not add to the window code's.
+__device__ __noinline__ unsigned long long svc_claim(const uint2* items0, const uint2* items1,
+                                                     const volatile unsigned long long* tail0,
+                                                     const volatile unsigned long long* tail1,
+                                                     unsigned long long* head0, unsigned long long* head1,
+                                                     unsigned long long ring_mask, const volatile unsigned int* stop,
+                                                     unsigned long long idle_ns) {
+    const unsigned long long t0 = global_ns();
+    unsigned int nap = 256;
+    for (;;) {
+        if (ld_acquire_sys32(stop)) return ~0ull;
+        for (int q = 0; q < 2; ++q) {
+            unsigned long long* head = q ? head1 : head0;
+            const unsigned long long t = ld_acquire_sys(q ? tail1 : tail0);
+            unsigned long long h = *reinterpret_cast<volatile unsigned long long*>(head);
+            while (h < t) {
+                const unsigned long long prev = atomicCAS(head, h, h + 1);
+                if (prev == h) {
+                    const volatile unsigned int* it =
+                        reinterpret_cast<const volatile unsigned int*>((q ? items1 : items0) + (h & ring_mask));
+                    return (static_cast<unsigned long long>(it[0]) << 32) | it[1];
+                }
+                h = prev;
+            }
+        }
+        if (global_ns() - t0 > idle_ns) return ~0ull;
+        __nanosleep(nap);
+        nap = nap < 16384 ? nap * 2 : nap;
+    }
+}
+
+// Persistent consensus over the shared queue: each warp owns one scratch
+// slot and takes windows of any job until the queue stays empty. Sized for
+// at most kSvcCtasPerSm resident CTAs per SM, so that the rest of each SM
+// stays free for the alignment and layer kernels of newly admitted jobs.
+constexpr int kSvcCtasPerSm = 3;
+__global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_kernel(PoaSvcArgs s) {
+    __shared__ PoaShared sh_all[kWarpsPerCta];
+    __shared__ Graph g_all[kWarpsPerCta];
+    __shared__ PoaArgs a_all[kWarpsPerCta];
+    extern __shared__ int4 ring_all[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int4* ring = ring_all + wid * (kRingBytesPerWarp / 16);
+    PoaShared& sh = sh_all[wid];
+    const uint32_t slot = blockIdx.x * kWarpsPerCta + wid;
+    if (lane == 0) g_all[wid] = make_graph(s.base, slot);
+    __syncwarp();
+    for (;;) {
+        unsigned long long it = 0;
+        if (lane == 0)
+            it = svc_claim(s.items[0], s.items[1], s.tail[0], s.tail[1], s.head[0], s.head[1], s.ring_mask, s.stop,
+                           s.idle_ns);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it == ~0ull) break;
+        const uint32_t job = uint32_t(it >> 32), win = uint32_t(it);
+        if (lane == 0) {
+            const PoaJobDev& J = s.jobs[job];
+            PoaArgs a = s.base;
+            a.in = J.in;
+            a.wins = J.wins;
+            a.layers = J.layers;
+            a.out = J.out;
+            a.out_len = J.out_len;
+            a.flags = J.flags;
+            a.trim = J.trim;
+            a.cells = J.cells;
+            a.nwin = J.total;
+            a_all[wid] = a;
+        }
+        __syncwarp();
+        poa_window(a_all[wid], g_all[wid], sh, win, lane, ring);
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) {
+            const PoaJobDev& J = s.jobs[job];
+            const unsigned int d = atomicAdd(&s.done[job], 1u) + 1u;
+            if (d == J.total) {
+                __threadfence_system();
+                s.finished[job] = J.generation;
+            }
+        }
+    }
 }
 
 }  // namespace
@@ -2575,26 +2726,43 @@ void PoaEngine::forget() {
     layers_ptr_ = nullptr;
 }
 
-void PoaEngine::run(bool plain) {
+void PoaEngine::prepare_outputs() {
     const size_t n = nwin_;
     stats_.launches = 0;
     stats_.items = n;
     stats_.cells = 0;
+    stats_.edge_cells = 0;
     stats_.kernel_ms = 0;
+    stats_.top_kernel_ms = 0;
     if (n == 0) return;
     d_out_.reserve(std::max<uint64_t>(out_cap_, 16));
     d_outlen_.reserve(n * 4);
     d_flags_.reserve(n);
     d_misc_.reserve(64);
+}
+
+void PoaEngine::run(bool plain) {
+    prepare_outputs();
+    const size_t n = nwin_;
+    if (n == 0) return;
     std::vector<uint32_t> todo(n);
     const uint32_t* h_order = h_order_.as<uint32_t>();
-    // batched form: size-sorted queue; plain form: input order
+    // batched form: size-sorted queue (heaviest first, or size buckets
+    // interleaved by the device's tuning); plain form: input order
+    const rb_tuning tune = tuning_get(dev_.device);
     for (size_t i = 0; i < n; ++i) todo[i] = plain ? uint32_t(i) : h_order[i];
+    if (!plain && tune.consensus_order == 1)
+        for (size_t i = 0, lo = 0, hi = n; i < n; ++i) todo[i] = h_order[(i & 1) ? --hi : lo++];
     // starting graph capacity; windows that outgrow it run again with four
     // times as much. RB_POA_NCAP lowers the start (tests of the retry path);
     // results do not depend on it.
     int ncap = 4096;
     if (const char* e = getenv("RB_POA_NCAP")) ncap = std::max(256, std::min(4096, atoi(e)));
+    run_list(std::move(todo), ncap, plain);
+}
+
+void PoaEngine::run_list(std::vector<uint32_t> todo, int ncap, bool plain) {
+    const size_t n = nwin_;
     std::vector<uint8_t> flags(n);
     float total_ms = 0;
     // DP row width: every layer's columns rounded up to whole warp passes
@@ -2606,9 +2774,11 @@ void PoaEngine::run(bool plain) {
         // resident windows (one warp each): enough to fill the SMs, bounded by
         // a scratch budget
         const size_t budget = scratch_budget_;
-        // resident windows: the context's share of the SMs (all by default)
+        // resident windows: the device's tuned CTAs per SM on the context's
+        // share of the SMs (all by default)
+        const uint32_t cps = std::min<uint32_t>(kCtasPerSm, tuning_get(dev_.device).consensus_ctas_per_sm);
         const size_t resident = std::max<size_t>(
-            kWarpsPerCta, size_t(dev_.sm_count) * kWarpsPerCta * kCtasPerSm * sm_share_pct_ / 100);
+            kWarpsPerCta, size_t(dev_.sm_count) * kWarpsPerCta * cps * sm_share_pct_ / 100);
         size_t slots = std::min<size_t>(todo.size(), plain ? todo.size() : resident);
         // RB_POA_SLOTS caps the resident windows (smaller scratch, e.g. for
         // profiler captures); results do not depend on it
@@ -2674,15 +2844,16 @@ void PoaEngine::run(bool plain) {
             }
         }
         check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
-        unsigned long long cells = 0;
-        check_cuda(cudaMemcpyAsync(&cells, a.cells, 8, cudaMemcpyDeviceToHost, stream_), "D2H cells");
+        unsigned long long cells[2] = {0, 0};
+        check_cuda(cudaMemcpyAsync(cells, a.cells, 16, cudaMemcpyDeviceToHost, stream_), "D2H cells");
         check_cuda(cudaMemcpyAsync(flags.data(), d_flags_.ptr, n, cudaMemcpyDeviceToHost, stream_), "D2H flags");
         check_cuda(cudaStreamSynchronize(stream_), "poa sync");
         check_cuda(cudaGetLastError(), "poa kernel");
         float ms = 0;
         cudaEventElapsedTime(&ms, ev0_, ev1_);
         total_ms += ms;
-        stats_.cells += cells;
+        stats_.cells += cells[0];
+        stats_.edge_cells += cells[1];
         std::vector<uint32_t> again;
         for (uint32_t w : todo) {
             if (flags[w] & kFailed) throw Error{RB_ERR_DEVICE, "rb_poa: window consensus failed on the device"};
@@ -2694,8 +2865,8 @@ void PoaEngine::run(bool plain) {
         }
         todo.swap(again);
     }
-    stats_.kernel_ms = total_ms;
-    stats_.top_kernel_ms = total_ms;
+    stats_.kernel_ms += total_ms;
+    stats_.top_kernel_ms += total_ms;
     stats_.max_nodes = uint32_t(ncap);
 }
 
@@ -2734,6 +2905,309 @@ void PoaEngine::fetch(rb_poa_result* out) {
     out->consensus = cons_.data();
     out->offsets = offsets_.data();
     out->polished = polished_.data();
+}
+
+}  // namespace rb
+
+// ---------------------------------------------------------------------------
+// Shared window-consensus service (continuous batching for the serving loop)
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
+
+namespace rb {
+
+namespace {
+constexpr uint32_t kSvcJobs = 256;                  // concurrent batches
+constexpr unsigned long long kSvcRing = 1ull << 21; // items per priority ring
+}  // namespace
+
+struct PoaSvcState {
+    int device = 0;
+    DeviceInfo dev;
+    cudaStream_t stream = nullptr;     // the persistent kernel's stream
+    cudaStream_t ctl = nullptr;        // small control copies
+    cudaEvent_t done_ev = nullptr;
+    PoaSvcArgs args{};
+    DevBuf d_scratch, d_head, d_done;
+    PoaJobDev* h_jobs = nullptr;       // mapped
+    uint2* h_items[2] = {nullptr, nullptr};
+    unsigned long long* h_tail = nullptr;  // [2], mapped
+    unsigned int* h_finished = nullptr;    // [kSvcJobs], mapped
+    unsigned int* h_stop = nullptr;        // mapped
+    uint32_t slots = 0, grid = 0;
+    std::mutex mu;
+    std::condition_variable cv, cv_slot;
+    std::vector<uint32_t> free_jobs;
+    std::vector<uint32_t> generation;
+    unsigned long long published[2] = {0, 0};
+    unsigned long long active_items = 0;
+    bool running = false, stopping = false;
+    std::string error;
+    uint32_t launches = 0;
+    std::thread thread;
+};
+
+PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window_length, size_t scratch_budget,
+                       uint32_t ctas_per_sm)
+    : st_(new PoaSvcState()) {
+    PoaSvcState& S = *st_;
+    S.device = device;
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    S.dev.device = device;
+    check_cuda(cudaDeviceGetAttribute(&S.dev.sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
+    check_cuda(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaStreamCreateWithFlags(&S.ctl, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaEventCreateWithFlags(&S.done_ev, cudaEventDisableTiming), "cudaEventCreate");
+    // slot layout for layers up to three window lengths; longer ones (and
+    // graphs over 4096 nodes) overflow and run again in the job's own engine
+    const int ncap = 4096, ecap = 2 * ncap, acap = ncap;
+    const int lcap = row_cover(int(std::max<uint32_t>(window_length, 1)) * 3 + 1);
+    const size_t slot = walk_layout(ncap, ecap, acap, lcap, [](int, size_t) {});
+    const uint32_t cps = std::max<uint32_t>(1, std::min<uint32_t>(ctas_per_sm, kSvcCtasPerSm));
+    size_t slots = size_t(S.dev.sm_count) * cps * kWarpsPerCta;
+    while (slots > kWarpsPerCta && slots * slot > scratch_budget) slots -= kWarpsPerCta;
+    S.slots = uint32_t(slots);
+    S.grid = uint32_t(slots / kWarpsPerCta);
+    {
+        AllocStreamScope none(nullptr);
+        S.d_scratch.release();
+    }
+    check_cuda(cudaMalloc(&S.d_scratch.ptr, slots * slot), "cudaMalloc service scratch");
+    S.d_scratch.bytes = slots * slot;
+    check_cuda(cudaMalloc(&S.d_head.ptr, 64), "cudaMalloc");
+    S.d_head.bytes = 64;
+    check_cuda(cudaMalloc(&S.d_done.ptr, kSvcJobs * 4), "cudaMalloc");
+    S.d_done.bytes = kSvcJobs * 4;
+    check_cuda(cudaMemset(S.d_head.ptr, 0, 64), "cudaMemset");
+    check_cuda(cudaMemset(S.d_done.ptr, 0, kSvcJobs * 4), "cudaMemset");
+    auto mapped = [](void** p, size_t b) {
+        check_cuda(cudaHostAlloc(p, b, cudaHostAllocMapped | cudaHostAllocPortable), "cudaHostAlloc mapped");
+        memset(*p, 0, b);
+    };
+    mapped(reinterpret_cast<void**>(&S.h_jobs), sizeof(PoaJobDev) * kSvcJobs);
+    mapped(reinterpret_cast<void**>(&S.h_items[0]), sizeof(uint2) * kSvcRing);
+    mapped(reinterpret_cast<void**>(&S.h_items[1]), sizeof(uint2) * kSvcRing);
+    mapped(reinterpret_cast<void**>(&S.h_tail), 64);
+    mapped(reinterpret_cast<void**>(&S.h_finished), 4 * kSvcJobs);
+    mapped(reinterpret_cast<void**>(&S.h_stop), 64);
+    auto dev_of = [](void* h) {
+        void* d = nullptr;
+        check_cuda(cudaHostGetDevicePointer(&d, h, 0), "cudaHostGetDevicePointer");
+        return d;
+    };
+    PoaSvcArgs& A = S.args;
+    memset(&A, 0, sizeof(A));
+    A.base.scratch = S.d_scratch.as<uint8_t>();
+    A.base.slot_bytes = slot;
+    A.base.ncap = ncap;
+    A.base.ecap = ecap;
+    A.base.acap = acap;
+    A.base.lcap = lcap;
+    A.base.match = m;
+    A.base.mismatch = x;
+    A.base.gap = g;
+    A.jobs = static_cast<const PoaJobDev*>(dev_of(S.h_jobs));
+    A.items[0] = static_cast<const uint2*>(dev_of(S.h_items[0]));
+    A.items[1] = static_cast<const uint2*>(dev_of(S.h_items[1]));
+    unsigned long long* dtail = static_cast<unsigned long long*>(dev_of(S.h_tail));
+    A.tail[0] = dtail;
+    A.tail[1] = dtail + 1;
+    A.head[0] = S.d_head.as<unsigned long long>();
+    A.head[1] = S.d_head.as<unsigned long long>() + 1;
+    A.ring_mask = kSvcRing - 1;
+    A.done = S.d_done.as<unsigned int>();
+    A.finished = static_cast<unsigned int*>(dev_of(S.h_finished));
+    A.stop = static_cast<const unsigned int*>(dev_of(S.h_stop));
+    A.idle_ns = 3000000ull;  // 3 ms
+    for (uint32_t j = kSvcJobs; j-- > 0;) S.free_jobs.push_back(j);
+    S.generation.assign(kSvcJobs, 0);
+    check_cuda(cudaFuncSetAttribute(poa_service_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kWarpsPerCta * kRingBytesPerWarp),
+               "cudaFuncSetAttribute");
+    S.thread = std::thread([this] { dispatcher(); });
+}
+
+PoaService::~PoaService() {
+    PoaSvcState& S = *st_;
+    {
+        std::lock_guard<std::mutex> lk(S.mu);
+        S.stopping = true;
+        *reinterpret_cast<volatile unsigned int*>(S.h_stop) = 1u;
+    }
+    S.cv.notify_all();
+    if (S.thread.joinable()) S.thread.join();
+    cudaSetDevice(S.device);
+    cudaStreamSynchronize(S.stream);
+    cudaStreamSynchronize(S.ctl);
+    cudaFree(S.d_scratch.ptr);
+    S.d_scratch.ptr = nullptr;
+    cudaFree(S.d_head.ptr);
+    S.d_head.ptr = nullptr;
+    cudaFree(S.d_done.ptr);
+    S.d_done.ptr = nullptr;
+    cudaFreeHost(S.h_jobs);
+    cudaFreeHost(S.h_items[0]);
+    cudaFreeHost(S.h_items[1]);
+    cudaFreeHost(S.h_tail);
+    cudaFreeHost(S.h_finished);
+    cudaFreeHost(S.h_stop);
+    cudaEventDestroy(S.done_ev);
+    cudaStreamDestroy(S.stream);
+    cudaStreamDestroy(S.ctl);
+    delete st_;
+}
+
+uint32_t PoaService::slots() const { return st_->slots; }
+uint32_t PoaService::launches() const { return st_->launches; }
+
+// Keeps the persistent kernel running while items are pending: after the
+// kernel leaves (idle, or racing a publish), items still unclaimed start a
+// new launch.
+void PoaService::dispatcher() {
+    PoaSvcState& S = *st_;
+    cudaSetDevice(S.device);
+    std::unique_lock<std::mutex> lk(S.mu);
+    while (!S.stopping) {
+        S.cv.wait_for(lk, std::chrono::microseconds(500));
+        if (S.stopping) break;
+        if (S.running) {
+            const cudaError_t q = cudaEventQuery(S.done_ev);
+            if (q == cudaErrorNotReady) continue;
+            S.running = false;
+            if (q != cudaSuccess) {
+                S.error = std::string("rb_poa service kernel: ") + cudaGetErrorString(q);
+                S.cv_slot.notify_all();
+                continue;
+            }
+        }
+        if (!S.error.empty()) continue;
+        if (S.published[0] + S.published[1] == 0) continue;
+        unsigned long long head[2] = {0, 0};
+        if (cudaMemcpyAsync(head, S.d_head.ptr, 16, cudaMemcpyDeviceToHost, S.ctl) != cudaSuccess ||
+            cudaStreamSynchronize(S.ctl) != cudaSuccess) {
+            S.error = "rb_poa service: head read failed";
+            S.cv_slot.notify_all();
+            continue;
+        }
+        if (head[0] >= S.published[0] && head[1] >= S.published[1]) continue;
+        poa_service_kernel<<<S.grid, 32 * kWarpsPerCta, kWarpsPerCta * kRingBytesPerWarp, S.stream>>>(S.args);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventRecord(S.done_ev, S.stream);
+        if (e != cudaSuccess) {
+            S.error = std::string("rb_poa service launch: ") + cudaGetErrorString(e);
+            S.cv_slot.notify_all();
+            continue;
+        }
+        S.running = true;
+        ++S.launches;
+    }
+}
+
+void PoaService::run_batch(const PoaJobDev& job, const uint32_t* order, size_t n, bool high_priority) {
+    PoaSvcState& S = *st_;
+    if (n == 0) return;
+    if (n > kSvcRing / 2) throw Error{RB_ERR_ARG, "rb_poa service: batch larger than the shared queue"};
+    uint32_t slot = 0, gen = 0;
+    {
+        std::unique_lock<std::mutex> lk(S.mu);
+        // a job slot, and room in the rings for every item not yet finished
+        S.cv_slot.wait(lk, [&] {
+            return !S.error.empty() || S.stopping ||
+                   (!S.free_jobs.empty() && S.active_items + n <= kSvcRing / 2);
+        });
+        if (!S.error.empty()) throw Error{RB_ERR_DEVICE, S.error};
+        if (S.stopping) throw Error{RB_ERR_ARG, "rb_poa service: shutting down"};
+        slot = S.free_jobs.back();
+        S.free_jobs.pop_back();
+        S.active_items += n;
+        gen = ++S.generation[slot];
+    }
+    // the slot's done counter starts from zero before any item is visible
+    check_cuda(cudaMemsetAsync(S.d_done.as<unsigned int>() + slot, 0, 4, S.ctl), "memset done");
+    check_cuda(cudaStreamSynchronize(S.ctl), "service control sync");
+    {
+        std::lock_guard<std::mutex> lk(S.mu);
+        PoaJobDev rec = job;
+        rec.total = uint32_t(n);
+        rec.generation = gen;
+        S.h_jobs[slot] = rec;
+        const int q = high_priority ? 0 : 1;
+        uint2* ring = S.h_items[q];
+        unsigned long long t = S.published[q];
+        for (size_t i = 0; i < n; ++i) ring[(t + i) & (kSvcRing - 1)] = make_uint2(slot, order[i]);
+        S.published[q] = t + n;
+        std::atomic_thread_fence(std::memory_order_release);
+        reinterpret_cast<volatile unsigned long long*>(S.h_tail)[q] = t + n;
+        std::atomic_thread_fence(std::memory_order_seq_cst);
+    }
+    S.cv.notify_all();
+    // wait for the batch; the dispatcher keeps a kernel running meanwhile
+    volatile unsigned int* fin = S.h_finished + slot;
+    std::string err;
+    for (;;) {
+        if (*fin == gen) break;
+        {
+            std::lock_guard<std::mutex> lk(S.mu);
+            if (!S.error.empty()) {
+                err = S.error;
+                break;
+            }
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    {
+        std::lock_guard<std::mutex> lk(S.mu);
+        if (err.empty()) {
+            S.free_jobs.push_back(slot);
+            S.active_items -= n;
+        }
+    }
+    S.cv_slot.notify_all();
+    if (!err.empty()) throw Error{RB_ERR_DEVICE, err};
+}
+
+void PoaEngine::run_shared(PoaService& svc, bool high_priority) {
+    prepare_outputs();
+    const size_t n = nwin_;
+    if (n == 0) return;
+    check_cuda(cudaMemsetAsync(d_misc_.ptr, 0, 64, stream_), "memset counters");
+    // the batch's inputs and descriptors are complete on this engine's stream
+    check_cuda(cudaStreamSynchronize(stream_), "poa stage sync");
+    PoaJobDev job;
+    memset(&job, 0, sizeof(job));
+    job.in = in_ptr_;
+    job.wins = d_desc_.as<PoaWinDev>();
+    job.layers = layers_ptr_;
+    job.out = d_out_.as<char>();
+    job.out_len = d_outlen_.as<uint32_t>();
+    job.flags = d_flags_.as<uint8_t>();
+    job.cells = reinterpret_cast<unsigned long long*>(d_misc_.as<unsigned int>() + 8);
+    job.trim = trim_;
+    const auto t0 = std::chrono::steady_clock::now();
+    svc.run_batch(job, h_order_.as<uint32_t>(), n, high_priority);
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    std::vector<uint8_t> flags(n);
+    unsigned long long cells[2] = {0, 0};
+    check_cuda(cudaMemcpyAsync(flags.data(), d_flags_.ptr, n, cudaMemcpyDeviceToHost, stream_), "D2H flags");
+    check_cuda(cudaMemcpyAsync(cells, job.cells, 16, cudaMemcpyDeviceToHost, stream_), "D2H cells");
+    check_cuda(cudaStreamSynchronize(stream_), "poa sync");
+    stats_.cells = cells[0];
+    stats_.edge_cells = cells[1];
+    stats_.kernel_ms = ms;
+    stats_.top_kernel_ms = ms;
+    std::vector<uint32_t> again;
+    for (uint32_t w = 0; w < n; ++w) {
+        if (flags[w] & kFailed) throw Error{RB_ERR_DEVICE, "rb_poa: window consensus failed on the device"};
+        if (flags[w] & kOverflow) again.push_back(w);
+    }
+    // windows that outgrew the shared slots: this engine's own launch with
+    // four times the graph capacity (the same path a private run takes)
+    if (!again.empty()) run_list(std::move(again), 4 * 4096, false);
 }
 
 }  // namespace rb

@@ -2,6 +2,7 @@
 // device engines: argument checks, device selection, error codes.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -72,6 +73,46 @@ void HostBuf::release() {
     bytes = 0;
 }
 
+namespace {
+constexpr int kTuneDevices = 64;
+std::mutex g_tune_mu;
+rb_tuning g_tune[kTuneDevices];
+bool g_tune_init[kTuneDevices] = {false};
+
+rb_tuning tuning_default() {
+    rb_tuning t;
+    memset(&t, 0, sizeof(t));
+    t.consensus_ctas_per_sm = 3;
+    t.consensus_order = 0;
+    t.alignment_warps_per_sm = 16;
+    return t;
+}
+
+rb_tuning tuning_clamp(rb_tuning t) {
+    t.consensus_ctas_per_sm = std::max<uint32_t>(1, std::min<uint32_t>(3, t.consensus_ctas_per_sm));
+    t.consensus_order = t.consensus_order ? 1 : 0;
+    t.alignment_warps_per_sm = std::max<uint32_t>(4, std::min<uint32_t>(32, t.alignment_warps_per_sm & ~3u));
+    return t;
+}
+}  // namespace
+
+rb_tuning tuning_get(int device) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (device < 0 || device >= kTuneDevices) return tuning_default();
+    if (!g_tune_init[device]) {
+        g_tune[device] = tuning_default();
+        g_tune_init[device] = true;
+    }
+    return g_tune[device];
+}
+
+void tuning_set(int device, const rb_tuning& t) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (device < 0 || device >= kTuneDevices) return;
+    g_tune[device] = tuning_clamp(t);
+    g_tune_init[device] = true;
+}
+
 }  // namespace rb
 
 struct rb_ctx {
@@ -83,12 +124,19 @@ struct rb_ctx {
     std::unique_ptr<rb::NwEngine> nw;
     std::unique_ptr<rb::PoaEngine> poa;
     std::unique_ptr<rb::LayerEngine> layers;
+    rb::PoaService* svc = nullptr;       // shared consensus kernel (serving), not owned
+    uint32_t svc_priority_windows = 0;
     std::string err;
 };
 
 namespace rb {
 void ctx_set_poa_budget(rb_ctx* ctx, size_t bytes) {
     if (ctx && ctx->poa) ctx->poa->set_scratch_budget(bytes);
+}
+void ctx_set_poa_service(rb_ctx* ctx, PoaService* svc, uint32_t priority_windows) {
+    if (!ctx) return;
+    ctx->svc = svc;
+    ctx->svc_priority_windows = priority_windows;
 }
 }  // namespace rb
 
@@ -222,7 +270,12 @@ int rb_poa_stage(rb_ctx* ctx, const rb_window* windows, size_t n, int trim) {
     return guarded(ctx, [&]() { ctx->poa->stage(windows, n, trim); });
 }
 int rb_poa_run(rb_ctx* ctx) {
-    return guarded(ctx, [&]() { ctx->poa->run(); });
+    return guarded(ctx, [&]() {
+        if (ctx->svc)
+            ctx->poa->run_shared(*ctx->svc, ctx->poa->staged() <= ctx->svc_priority_windows);
+        else
+            ctx->poa->run();
+    });
 }
 
 int rb_poa_run_plain(rb_ctx* ctx) {
@@ -312,5 +365,98 @@ int rb_align_stats(const rb_ctx* ctx, rb_stats* out) {
 }
 
 void rb_free(void* p) { free(p); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- autotuner
+
+extern "C" {
+
+int rb_tuning_get(int device, rb_tuning* out) {
+    if (!out) return RB_ERR_ARG;
+    *out = rb::tuning_get(device);
+    return RB_OK;
+}
+
+int rb_tuning_set(int device, const rb_tuning* in) {
+    if (!in) return RB_ERR_ARG;
+    rb::tuning_set(device, *in);
+    return RB_OK;
+}
+
+int rb_autotune(rb_ctx* ctx, int what) {
+    return guarded(ctx, [&]() {
+        const int dev = ctx->dev.device;
+        rb_tuning best = rb::tuning_get(dev);
+        if (what & 1) {
+            if (ctx->poa->staged() == 0) throw rb::Error{RB_ERR_ARG, "rb_autotune: no windows staged"};
+            double best_ms = 1e300;
+            std::string ref;
+            std::vector<uint8_t> ref_pol;
+            for (uint32_t cps = 3; cps >= 1; --cps) {
+                for (uint32_t order = 0; order <= 1; ++order) {
+                    rb_tuning t = best;
+                    t.consensus_ctas_per_sm = cps;
+                    t.consensus_order = order;
+                    rb::tuning_set(dev, t);
+                    ctx->poa->run();
+                    const double ms = ctx->poa->stats().kernel_ms;
+                    rb_poa_result r;
+                    ctx->poa->fetch(&r);
+                    const size_t n = ctx->poa->staged();
+                    std::string cons(r.consensus, r.consensus + r.offsets[n]);
+                    std::vector<uint8_t> pol(r.polished, r.polished + n);
+                    if (ref_pol.empty() && ref.empty()) {
+                        ref.swap(cons);
+                        ref_pol.swap(pol);
+                    } else if (cons != ref || pol != ref_pol) {
+                        rb::tuning_set(dev, best);
+                        throw rb::Error{RB_ERR_DEVICE, "rb_autotune: consensus differs between launch settings"};
+                    }
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best.consensus_ctas_per_sm = cps;
+                        best.consensus_order = order;
+                    }
+                }
+            }
+            best.consensus_ms = best_ms;
+            best.tuned |= 1u;
+        }
+        if (what & 2) {
+            if (ctx->nw->staged() == 0) throw rb::Error{RB_ERR_ARG, "rb_autotune: no pairs staged"};
+            double best_ms = 1e300;
+            std::vector<int32_t> ref_d;
+            std::vector<uint32_t> ref_bp;
+            const uint32_t cand[] = {8, 12, 16, 24, 32};
+            for (uint32_t w : cand) {
+                rb_tuning t = best;
+                t.alignment_warps_per_sm = w;
+                rb::tuning_set(dev, t);
+                ctx->nw->run();
+                const double ms = ctx->nw->stats().kernel_ms;
+                rb_aln_result r;
+                ctx->nw->fetch(&r);
+                const size_t n = ctx->nw->staged();
+                std::vector<int32_t> d(r.edit_distance, r.edit_distance + n);
+                std::vector<uint32_t> bp(r.breakpoints, r.breakpoints + r.bp_offsets[n]);
+                if (ref_d.empty()) {
+                    ref_d.swap(d);
+                    ref_bp.swap(bp);
+                } else if (d != ref_d || bp != ref_bp) {
+                    rb::tuning_set(dev, best);
+                    throw rb::Error{RB_ERR_DEVICE, "rb_autotune: alignments differ between launch settings"};
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best.alignment_warps_per_sm = w;
+                }
+            }
+            best.alignment_ms = best_ms;
+            best.tuned |= 2u;
+        }
+        rb::tuning_set(dev, best);
+    });
+}
 
 }  // extern "C"

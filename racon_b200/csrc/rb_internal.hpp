@@ -60,6 +60,10 @@ struct DeviceInfo {
     size_t smem_optin = 0;
 };
 
+// Launch choices of a device (rb_tuning), read by the engines at every run.
+rb_tuning tuning_get(int device);
+void tuning_set(int device, const rb_tuning& t);
+
 // ----- device sequence store (layers.cu) -----
 // One entry of the staged sequence table: offsets of the forward bases and
 // quality and of the reverse complement and reversed quality in the store.
@@ -115,6 +119,7 @@ public:
     void cigar_breakpoints(const rb_cigar_overlap* ovl, size_t n, uint32_t window_length,
                            rb_aln_result* out);
     const rb_stats& stats() const { return stats_; }
+    size_t staged() const { return npairs_; }
 
 private:
     void reserve_scratch(uint32_t max_m, uint32_t max_n);
@@ -164,6 +169,8 @@ struct PoaLayerDev {
     uint32_t len, begin, end, pad;
 };
 
+class PoaService;
+
 class PoaEngine {
 public:
     PoaEngine(const DeviceInfo& dev, cudaStream_t stream, int8_t m, int8_t x, int8_t g);
@@ -186,6 +193,11 @@ public:
     // percent of the SMs the persistent kernel fills (100: all)
     void set_sm_share(uint32_t pct) { sm_share_pct_ = pct ? pct : 100; }
     void run(bool plain = false);
+    // The staged windows through a device-wide shared queue (serving):
+    // returns when every window of this batch is done; windows that outgrow
+    // the shared slots run again here with larger graph capacity.
+    void run_shared(PoaService& svc, bool high_priority);
+    size_t staged() const { return nwin_; }
     void fetch(rb_poa_result* out);
     const rb_stats& stats() const { return stats_; }
     // device bytes the per-window scratch slots may take (resident windows
@@ -195,6 +207,9 @@ public:
     static size_t slot_bytes_for(uint32_t max_layer_length);
 
 private:
+    friend class PoaService;
+    void prepare_outputs();
+    void run_list(std::vector<uint32_t> todo, int ncap, bool plain);
     DeviceInfo dev_;
     cudaStream_t stream_;
     cudaEvent_t ev0_, ev1_, ev2_, ev3_;
@@ -217,6 +232,36 @@ private:
     std::vector<std::pair<uint64_t, uint32_t>> labels_;  // (id, rank) per window
     size_t scratch_budget_ = size_t(48) << 30;
     rb_stats stats_{};
+};
+
+// ----- shared window-consensus service (poa_consensus.cu) -----
+// Continuous batching for the serving loop: one persistent consensus kernel
+// per device whose warps pull (job, window) items from two host-mapped
+// queues (high priority first), so windows of jobs admitted while others run
+// start as soon as any warp frees up. Jobs append their items and wait for a
+// per-job completion flag; the kernel leaves after a bounded idle time and a
+// dispatcher thread relaunches it when items are pending. Thread-safe.
+struct PoaJobDev;
+struct PoaSvcState;
+
+class PoaService {
+public:
+    // ctas_per_sm: resident consensus CTAs (4 warps each) per SM, 1..3; the
+    // rest of the SM stays free for other kernels (alignment of new jobs).
+    PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window_length, size_t scratch_budget,
+               uint32_t ctas_per_sm);
+    ~PoaService();
+    PoaService(const PoaService&) = delete;
+    PoaService& operator=(const PoaService&) = delete;
+    // Enqueues windows order[0..n) of the batch described by `job` and waits
+    // until all of them are done. Throws rb::Error on device failure.
+    void run_batch(const PoaJobDev& job, const uint32_t* order, size_t n, bool high_priority);
+    uint32_t slots() const;
+    uint32_t launches() const;
+
+private:
+    void dispatcher();
+    PoaSvcState* st_;
 };
 
 // ----- device layer assembly (layers.cu) -----
@@ -278,5 +323,9 @@ private:
 // Caps the window-consensus scratch of a context (server workers share one
 // device); defined in rb_capi.cpp.
 void ctx_set_poa_budget(rb_ctx* ctx, size_t bytes);
+// Routes the context's rb_poa_run through a shared consensus service
+// (nullptr: its own kernel); batches of at most priority_windows windows use
+// the high-priority queue. Defined in rb_capi.cpp.
+void ctx_set_poa_service(rb_ctx* ctx, PoaService* svc, uint32_t priority_windows);
 
 }  // namespace rb

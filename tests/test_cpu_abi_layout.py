@@ -27,6 +27,7 @@ STRUCTS = {
     "rb_server_job": "_ServerJob",
     "rb_server_times": "ServerTimes",
     "rb_stats": "Stats",
+    "rb_tuning": "Tuning",
 }
 
 

@@ -1,6 +1,9 @@
 """Serving loop (rb_server_*): every job's FASTA is the same alone and in the
-mix, admission by footprint serialises jobs under a small budget, and a bad
-job fails alone without stopping the server."""
+mix (with the shared consensus kernel, jobs admitted while it runs; and with
+per-job kernels), admission by footprint serialises jobs under a small
+budget, and a bad job fails alone without stopping the server."""
+import time
+
 import pytest
 
 from conftest import lambda_path
@@ -55,3 +58,36 @@ def test_server_bad_job_fails_alone(native_lib):
         with pytest.raises(native_lib.RaconB200Error, match="unsupported format extension"):
             srv.wait(bad)
         assert srv.wait(good)[0] == want
+
+
+def test_server_jobs_join_running_kernel(native_lib, tmp_path):
+    """Continuous batching: a long job keeps the shared consensus kernel busy
+    while small jobs arrive one by one; each small job's windows join the
+    running kernel (high-priority queue) and every output equals the job run
+    alone, including the long one."""
+    from racon_b200 import synthetic
+    r, o, t, _ = synthetic.contig(str(tmp_path / "big"), 1, scale=0.08)
+    big_alone = native_lib.polish_files(r, o, t, match=5, mismatch=-4, gap=-8)
+    want = _alone(native_lib)
+    with native_lib.Server(0, workers=4, match=5, mismatch=-4, gap=-8, window_length=500,
+                           priority_windows=120) as srv:
+        tb = srv.submit(r, o, t)
+        small = []
+        for i, (rr, oo) in enumerate(JOBS * 2):
+            time.sleep(0.05)
+            small.append(srv.submit(lambda_path(rr), lambda_path(oo), lambda_path(TARGET)))
+        got_small = [srv.wait(x) for x in small]
+        got_big = srv.wait(tb)
+    assert got_big[0] == big_alone
+    for i, (fasta, _) in enumerate(got_small):
+        assert fasta == want[i % len(JOBS)], "small job %d differs in the mix" % i
+
+
+def test_server_private_kernels_match(native_lib):
+    """shared_consensus=False: each job launches its own consensus kernel;
+    same outputs."""
+    want = _alone(native_lib)
+    with native_lib.Server(0, workers=2, match=5, mismatch=-4, gap=-8, shared_consensus=False) as srv:
+        tickets = [srv.submit(lambda_path(r), lambda_path(o), lambda_path(TARGET)) for r, o in JOBS]
+        got = [srv.wait(x)[0] for x in tickets]
+    assert got == want
