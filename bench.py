@@ -59,6 +59,7 @@ def _args():
     p.add_argument("--cpu-sample", type=int, default=400, help="windows in the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="keep the default launch choices")
+    p.add_argument("--no-pipeline", action="store_true", help="skip the whole-job end-to-end comparison")
     p.add_argument("--data-dir", default=None)
     p.add_argument("--serving-jobs", type=int, default=12, help="config-4 jobs in the serving measurement "
                    "(0 = skip it)")
@@ -288,6 +289,31 @@ def run_serving(args, device, rates):
                           "latency_vs_isolated": {"p50": _pct(ratio, 50), "p99": _pct(ratio, 99)}})
         out["rates"] = sweep
     return out
+
+
+def run_pipeline(args, paths, m, x, g, w):
+    """The whole job end to end, as racon's wall time counts it (parse,
+    overlap alignment, layers, consensus, stitching, FASTA text): the device
+    path through rb_polish_files against the CPU oracle's pipeline on every
+    host thread, and the two FASTA outputs compared byte for byte."""
+    import racon_b200
+    import oracle
+    frag = args.config == 3
+    kw = dict(window_length=w, quality_threshold=10.0, error_threshold=0.3, match=m, mismatch=x, gap=g)
+    threads = os.cpu_count() or 1
+    racon_b200.polish_files(*paths, fragment=frag, drop_unpolished=not frag, threads=threads, **kw)  # warm
+    dev = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        got = racon_b200.polish_files(*paths, fragment=frag, drop_unpolished=not frag, threads=threads, **kw)
+        dev.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    want, stage_s, counts = oracle.polish(*paths, fragment=frag, drop_unpolished=not frag, threads=threads, **kw)
+    cpu_s = time.perf_counter() - t0
+    return {"device_s": min(dev), "oracle_s": cpu_s, "oracle_threads": threads, "speedup": cpu_s / min(dev),
+            "fasta_identical": got == want, "fasta_bytes": len(got),
+            "path": "rb_polish_files (parse -> device alignment -> device layers -> device consensus -> stitch) "
+                    "vs the CPU oracle's pipeline, wall time per job"}
 
 
 def _oracle_align(pairs, threads):
@@ -687,6 +713,8 @@ def main():
         out["compute"]["oracle_sample_edge_cells_per_cell"] = cpu_ecells / max(1, ccells)
     ctx.close()
     job.close()
+    if rank == 0 and world == 1 and not args.no_pipeline:
+        out["pipeline"] = run_pipeline(args, paths, m, x, g, w)
     if world == 1 and args.serving_jobs > 0:
         # config 4 serving loop at 80% of its measured peak (--config 4 sweeps the load)
         out["serving"] = run_serving(args, local, [0.8])

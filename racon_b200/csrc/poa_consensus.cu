@@ -1096,6 +1096,14 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
     int4* const dblk = ring + kRingDescOffset;
     const int4* const rowdesc = g.rowdesc;
     int4 pre = lane < ndp ? rowdesc[lane] : make_int4(0, 0, 0, 0);
+    // hv holds the previous row's final scores between iterations (row 0
+    // first), and left_prev that row's score left of the lane's segment: a
+    // row whose first predecessor is the row just computed (the common
+    // chain) reads both from registers instead of the ring and a shuffle
+    int hv[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) hv[k] = (j0 + k) * gap;
+    int left_prev = lane == 0 ? kNegInf : (j0 - 1) * gap;
     for (int i = 1; i <= ndp; ++i) {
         const int bi = (i - 1) & 31;
         if (bi == 0) {
@@ -1116,7 +1124,6 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
 #pragma unroll
         for (int q = 0; q < Q; ++q) sw[q] = __vcmpeq4(sc[q], cmask) & diff4;
         int T[S];
-        int hv[S];
         uint32_t dbit = 0;
         auto load_row = [&](int r) {
             if (r == 0) {
@@ -1138,31 +1145,40 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
             }
         };
         auto sbyte = [&](int k) -> int { return int((sw[k >> 2] >> (8 * (k & 3))) & 0xFFu); };
-        load_row(np == 0 ? 0 : p0);
         {
-            int left = __shfl_up_sync(kFull, hv[S - 1], 1);
-            if (lane == 0) left = kNegInf;
+            const int r0 = np == 0 ? 0 : p0;
+            int left = left_prev;
+            if (r0 != i - 1) {
+                load_row(r0);
+                left = __shfl_up_sync(kFull, hv[S - 1], 1);
+                if (lane == 0) left = kNegInf;
+            }
+            // decision bits gathered in four independent words (short chains)
+            uint32_t dq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 const int pv = k == 0 ? left : hv[k - 1];
                 const int dg = pv + mm + sbyte(k);
                 bool dge;
                 T[k] = __vibmax_s32(dg, hv[k] + gap, &dge);
-                dbit |= uint32_t(dge) << k;
+                dq[k & 3] |= uint32_t(dge) << k;
             }
+            dbit = (dq[0] | dq[1]) | (dq[2] | dq[3]);
         }
         for (int p = 1; p < np; ++p) {
             load_row(np > 3 ? pred_idx[d.x + p] : (p == 1 ? d.y : d.z));
             int left = __shfl_up_sync(kFull, hv[S - 1], 1);
             if (lane == 0) left = kNegInf;
+            uint32_t lq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 const int pv = k == 0 ? left : hv[k - 1];
                 const int mx = __viaddmax_s32(hv[k], gap, pv + mm + sbyte(k));
                 bool keep;
                 T[k] = __vibmax_s32(T[k], mx, &keep);
-                dbit &= ~(uint32_t(!keep) << k);
+                lq[k & 3] |= uint32_t(!keep) << k;
             }
+            dbit &= ~((lq[0] | lq[1]) | (lq[2] | lq[3]));
         }
         // horizontal term
         constexpr int C = S / 4;  // cells per sub-chain
@@ -1181,24 +1197,34 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         int x = agg[0];
 #pragma unroll
         for (int c = 1; c < 4; ++c) x = __viaddmax_s32(x, C * gap, agg[c]);
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(kFull, x, o);
-            if (lane >= o) x = __viaddmax_s32(y, o * S * gap, x);
+        // max-plus prefix of the lane aggregates, x_l = max(x_l, x_(l-1) +
+        // S * gap), one lane per round until no lane changes: monotone and
+        // bounded by the exact prefix, so the fixed point is that prefix.
+        // Horizontal runs rarely cross a whole lane segment, so most rows
+        // take one round instead of the five of a full scan.
+        for (int it = 0; it < 31; ++it) {
+            int y = __shfl_up_sync(kFull, x, 1);
+            if (lane == 0) y = kNegInf;
+            const int nx = __viaddmax_s32(y, S * gap, x);
+            const bool changed = nx != x;
+            x = nx;
+            if (!__any_sync(kFull, changed)) break;
         }
         int cin = __shfl_up_sync(kFull, x, 1);  // final value left of the segment
         if (lane == 0) cin = kNegInf;
-        uint32_t hbit = 0;
+        left_prev = cin;
+        uint32_t hq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int next = __viaddmax_s32(cin, C * gap, agg[c]);
 #pragma unroll
             for (int k = c * C; k < (c + 1) * C; ++k) {
                 hv[k] = __viaddmax_s32(cin, (k - c * C + 1) * gap, hv[k]);
-                hbit |= uint32_t(hv[k] > T[k]) << k;
+                hq[k & 3] |= uint32_t(hv[k] > T[k]) << k;
             }
             cin = next;
         }
+        const uint32_t hbit = (hq[0] | hq[1]) | (hq[2] | hq[3]);
         int4* dst_g = reinterpret_cast<int4*>(Hm + i * lc + j0);
         int4* dst_r = ring + (i % R) * Q * 32 + lane;
 #pragma unroll
@@ -2388,35 +2414,29 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) poa_plain_kerne
 
 // ---------------- shared queue (serving) ----------------
 
-// Loads with acquire semantics at system scope: the host publishes queue
-// items and job records in mapped host memory, then the tail.
-__device__ __forceinline__ unsigned long long ld_acquire_sys(const volatile unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.sys.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ unsigned int ld_acquire_sys32(const volatile unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
 
+// Queue state lives in device memory: the host writes job records, then
+// items, then the tail with copies in one stream (each copy starts after the
+// previous one completes), so a warp that sees the new tail in L2 finds the
+// items and records there too. Idle warps poll that L2 word, never host
+// memory: polling over the bus, or acquire loads at system scope, would slow
+// the warps still computing on the same SMs.
 struct PoaSvcArgs {
-    PoaArgs base;                                // scoring, capacities, scratch slots
-    const PoaJobDev* jobs;                       // mapped host: job records
-    const uint2* items[2];                       // mapped host rings: (job slot, window), [0] = high priority
-    const volatile unsigned long long* tail[2];  // mapped host: items published
-    unsigned long long* head[2];                 // device: items claimed
+    PoaArgs base;                    // scoring, capacities, scratch slots
+    const PoaJobDev* jobs;           // device: job records
+    const uint2* items[2];           // device rings: (job slot, window), [0] = high priority
+    const unsigned long long* tail;  // device: [2] items published
+    unsigned long long* head;        // device: [2] items claimed
     unsigned long long ring_mask;
-    unsigned int* done;                          // device: windows finished per job slot
-    volatile unsigned int* finished;             // mapped host: generation of the last finished batch per slot
-    const volatile unsigned int* stop;           // mapped host: leave now
-    unsigned long long idle_ns;                  // a warp leaves after this long without work
+    unsigned int* done;              // device: windows finished per job slot
+    volatile unsigned int* finished; // mapped host: generation of the last finished batch per slot
+    const unsigned int* stop;        // device: leave now
+    unsigned long long idle_ns;      // a warp leaves after this long without work
 };
 
 // Claims the next item, high-priority ring first: returns (job << 32) |
@@ -2424,22 +2444,20 @@ struct PoaSvcArgs {
 // kernel always ends). Out of line with scalar arguments, so its registers
 // do not add to the window code's.
 __device__ __noinline__ unsigned long long svc_claim(const uint2* items0, const uint2* items1,
-                                                     const volatile unsigned long long* tail0,
-                                                     const volatile unsigned long long* tail1,
-                                                     unsigned long long* head0, unsigned long long* head1,
-                                                     unsigned long long ring_mask, const volatile unsigned int* stop,
+                                                     const unsigned long long* tail, unsigned long long* head,
+                                                     unsigned long long ring_mask, const unsigned int* stop,
                                                      unsigned long long idle_ns) {
     const unsigned long long t0 = global_ns();
-    unsigned int nap = 256;
+    unsigned int nap = 512;
     for (;;) {
-        if (ld_acquire_sys32(stop)) return ~0ull;
+        if (*reinterpret_cast<const volatile unsigned int*>(stop)) return ~0ull;
         for (int q = 0; q < 2; ++q) {
-            unsigned long long* head = q ? head1 : head0;
-            const unsigned long long t = ld_acquire_sys(q ? tail1 : tail0);
-            unsigned long long h = *reinterpret_cast<volatile unsigned long long*>(head);
+            const unsigned long long t = reinterpret_cast<const volatile unsigned long long*>(tail)[q];
+            unsigned long long h = reinterpret_cast<volatile unsigned long long*>(head)[q];
             while (h < t) {
-                const unsigned long long prev = atomicCAS(head, h, h + 1);
+                const unsigned long long prev = atomicCAS(head + q, h, h + 1);
                 if (prev == h) {
+                    __threadfence();
                     const volatile unsigned int* it =
                         reinterpret_cast<const volatile unsigned int*>((q ? items1 : items0) + (h & ring_mask));
                     return (static_cast<unsigned long long>(it[0]) << 32) | it[1];
@@ -2449,7 +2467,7 @@ __device__ __noinline__ unsigned long long svc_claim(const uint2* items0, const 
         }
         if (global_ns() - t0 > idle_ns) return ~0ull;
         __nanosleep(nap);
-        nap = nap < 16384 ? nap * 2 : nap;
+        nap = nap < 32768 ? nap * 2 : nap;
     }
 }
 
@@ -2472,23 +2490,27 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
     for (;;) {
         unsigned long long it = 0;
         if (lane == 0)
-            it = svc_claim(s.items[0], s.items[1], s.tail[0], s.tail[1], s.head[0], s.head[1], s.ring_mask, s.stop,
-                           s.idle_ns);
+            it = svc_claim(s.items[0], s.items[1], s.tail, s.head, s.ring_mask, s.stop, s.idle_ns);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it == ~0ull) break;
         const uint32_t job = uint32_t(it >> 32), win = uint32_t(it);
+        uint32_t total = 0, gen = 0;
         if (lane == 0) {
-            const PoaJobDev& J = s.jobs[job];
+            // the record is rewritten for every batch that reuses the slot:
+            // read it past L1
+            const volatile PoaJobDev& J = s.jobs[job];
             PoaArgs a = s.base;
-            a.in = J.in;
-            a.wins = J.wins;
-            a.layers = J.layers;
-            a.out = J.out;
-            a.out_len = J.out_len;
-            a.flags = J.flags;
+            a.in = const_cast<const uint8_t*>(J.in);
+            a.wins = const_cast<const PoaWinDev*>(J.wins);
+            a.layers = const_cast<const PoaLayerDev*>(J.layers);
+            a.out = const_cast<char*>(J.out);
+            a.out_len = const_cast<uint32_t*>(J.out_len);
+            a.flags = const_cast<uint8_t*>(J.flags);
             a.trim = J.trim;
-            a.cells = J.cells;
-            a.nwin = J.total;
+            a.cells = const_cast<unsigned long long*>(J.cells);
+            total = J.total;
+            gen = J.generation;
+            a.nwin = total;
             a_all[wid] = a;
         }
         __syncwarp();
@@ -2496,11 +2518,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
         __threadfence();
         __syncwarp();
         if (lane == 0) {
-            const PoaJobDev& J = s.jobs[job];
             const unsigned int d = atomicAdd(&s.done[job], 1u) + 1u;
-            if (d == J.total) {
+            if (d == total) {
                 __threadfence_system();
-                s.finished[job] = J.generation;
+                s.finished[job] = gen;
             }
         }
     }
@@ -2929,17 +2950,24 @@ struct PoaSvcState {
     int device = 0;
     DeviceInfo dev;
     cudaStream_t stream = nullptr;     // the persistent kernel's stream
-    cudaStream_t ctl = nullptr;        // small control copies
+    cudaStream_t ctl = nullptr;        // queue writes and head reads (ordered copies)
     cudaEvent_t done_ev = nullptr;
     PoaSvcArgs args{};
-    DevBuf d_scratch, d_head, d_done;
-    PoaJobDev* h_jobs = nullptr;       // mapped
-    uint2* h_items[2] = {nullptr, nullptr};
-    unsigned long long* h_tail = nullptr;  // [2], mapped
-    unsigned int* h_finished = nullptr;    // [kSvcJobs], mapped
-    unsigned int* h_stop = nullptr;        // mapped
+    // device: scratch slots, queue rings, [tail0, tail1, head0, head1, stop],
+    // job records, per-job done counters
+    void* d_scratch = nullptr;
+    uint2* d_items[2] = {nullptr, nullptr};
+    unsigned long long* d_ctl = nullptr;
+    PoaJobDev* d_jobs = nullptr;
+    unsigned int* d_done = nullptr;
+    // host: pinned staging for the copies, mapped finished flags
+    uint2* h_stage = nullptr;               // kSvcRing / 2 items
+    PoaJobDev* h_rec = nullptr;             // one record
+    unsigned long long* h_val = nullptr;    // tail / stop values
+    unsigned int* h_finished = nullptr;     // [kSvcJobs], mapped
     uint32_t slots = 0, grid = 0;
-    std::mutex mu;
+    std::mutex mu;       // queue state, dispatcher
+    std::mutex pub_mu;   // publishing (staging buffers and the control stream)
     std::condition_variable cv, cv_slot;
     std::vector<uint32_t> free_jobs;
     std::vector<uint32_t> generation;
@@ -2972,36 +3000,26 @@ PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window
     while (slots > kWarpsPerCta && slots * slot > scratch_budget) slots -= kWarpsPerCta;
     S.slots = uint32_t(slots);
     S.grid = uint32_t(slots / kWarpsPerCta);
-    {
-        AllocStreamScope none(nullptr);
-        S.d_scratch.release();
-    }
-    check_cuda(cudaMalloc(&S.d_scratch.ptr, slots * slot), "cudaMalloc service scratch");
-    S.d_scratch.bytes = slots * slot;
-    check_cuda(cudaMalloc(&S.d_head.ptr, 64), "cudaMalloc");
-    S.d_head.bytes = 64;
-    check_cuda(cudaMalloc(&S.d_done.ptr, kSvcJobs * 4), "cudaMalloc");
-    S.d_done.bytes = kSvcJobs * 4;
-    check_cuda(cudaMemset(S.d_head.ptr, 0, 64), "cudaMemset");
-    check_cuda(cudaMemset(S.d_done.ptr, 0, kSvcJobs * 4), "cudaMemset");
-    auto mapped = [](void** p, size_t b) {
-        check_cuda(cudaHostAlloc(p, b, cudaHostAllocMapped | cudaHostAllocPortable), "cudaHostAlloc mapped");
-        memset(*p, 0, b);
-    };
-    mapped(reinterpret_cast<void**>(&S.h_jobs), sizeof(PoaJobDev) * kSvcJobs);
-    mapped(reinterpret_cast<void**>(&S.h_items[0]), sizeof(uint2) * kSvcRing);
-    mapped(reinterpret_cast<void**>(&S.h_items[1]), sizeof(uint2) * kSvcRing);
-    mapped(reinterpret_cast<void**>(&S.h_tail), 64);
-    mapped(reinterpret_cast<void**>(&S.h_finished), 4 * kSvcJobs);
-    mapped(reinterpret_cast<void**>(&S.h_stop), 64);
-    auto dev_of = [](void* h) {
-        void* d = nullptr;
-        check_cuda(cudaHostGetDevicePointer(&d, h, 0), "cudaHostGetDevicePointer");
-        return d;
-    };
+    check_cuda(cudaMalloc(&S.d_scratch, slots * slot), "cudaMalloc service scratch");
+    check_cuda(cudaMalloc(&S.d_items[0], sizeof(uint2) * kSvcRing), "cudaMalloc service queue");
+    check_cuda(cudaMalloc(&S.d_items[1], sizeof(uint2) * kSvcRing), "cudaMalloc service queue");
+    check_cuda(cudaMalloc(&S.d_ctl, 64), "cudaMalloc");
+    check_cuda(cudaMalloc(&S.d_jobs, sizeof(PoaJobDev) * kSvcJobs), "cudaMalloc");
+    check_cuda(cudaMalloc(&S.d_done, kSvcJobs * 4), "cudaMalloc");
+    check_cuda(cudaMemset(S.d_ctl, 0, 64), "cudaMemset");
+    check_cuda(cudaMemset(S.d_done, 0, kSvcJobs * 4), "cudaMemset");
+    check_cuda(cudaMemset(S.d_jobs, 0, sizeof(PoaJobDev) * kSvcJobs), "cudaMemset");
+    check_cuda(cudaMallocHost(&S.h_stage, sizeof(uint2) * (kSvcRing / 2)), "cudaMallocHost");
+    check_cuda(cudaMallocHost(&S.h_rec, sizeof(PoaJobDev)), "cudaMallocHost");
+    check_cuda(cudaMallocHost(&S.h_val, 64), "cudaMallocHost");
+    check_cuda(cudaHostAlloc(&S.h_finished, 4 * kSvcJobs, cudaHostAllocMapped | cudaHostAllocPortable),
+               "cudaHostAlloc mapped");
+    memset(S.h_finished, 0, 4 * kSvcJobs);
+    void* d_fin = nullptr;
+    check_cuda(cudaHostGetDevicePointer(&d_fin, S.h_finished, 0), "cudaHostGetDevicePointer");
     PoaSvcArgs& A = S.args;
     memset(&A, 0, sizeof(A));
-    A.base.scratch = S.d_scratch.as<uint8_t>();
+    A.base.scratch = static_cast<uint8_t*>(S.d_scratch);
     A.base.slot_bytes = slot;
     A.base.ncap = ncap;
     A.base.ecap = ecap;
@@ -3010,18 +3028,15 @@ PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window
     A.base.match = m;
     A.base.mismatch = x;
     A.base.gap = g;
-    A.jobs = static_cast<const PoaJobDev*>(dev_of(S.h_jobs));
-    A.items[0] = static_cast<const uint2*>(dev_of(S.h_items[0]));
-    A.items[1] = static_cast<const uint2*>(dev_of(S.h_items[1]));
-    unsigned long long* dtail = static_cast<unsigned long long*>(dev_of(S.h_tail));
-    A.tail[0] = dtail;
-    A.tail[1] = dtail + 1;
-    A.head[0] = S.d_head.as<unsigned long long>();
-    A.head[1] = S.d_head.as<unsigned long long>() + 1;
+    A.jobs = S.d_jobs;
+    A.items[0] = S.d_items[0];
+    A.items[1] = S.d_items[1];
+    A.tail = S.d_ctl;
+    A.head = S.d_ctl + 2;
+    A.stop = reinterpret_cast<const unsigned int*>(S.d_ctl + 4);
     A.ring_mask = kSvcRing - 1;
-    A.done = S.d_done.as<unsigned int>();
-    A.finished = static_cast<unsigned int*>(dev_of(S.h_finished));
-    A.stop = static_cast<const unsigned int*>(dev_of(S.h_stop));
+    A.done = S.d_done;
+    A.finished = static_cast<unsigned int*>(d_fin);
     A.idle_ns = 3000000ull;  // 3 ms
     for (uint32_t j = kSvcJobs; j-- > 0;) S.free_jobs.push_back(j);
     S.generation.assign(kSvcJobs, 0);
@@ -3036,25 +3051,29 @@ PoaService::~PoaService() {
     {
         std::lock_guard<std::mutex> lk(S.mu);
         S.stopping = true;
-        *reinterpret_cast<volatile unsigned int*>(S.h_stop) = 1u;
     }
     S.cv.notify_all();
+    S.cv_slot.notify_all();
     if (S.thread.joinable()) S.thread.join();
     cudaSetDevice(S.device);
+    {
+        // the stop word ends a running kernel within its idle bound
+        std::lock_guard<std::mutex> lk(S.pub_mu);
+        S.h_val[4] = 1;
+        cudaMemcpyAsync(S.d_ctl + 4, S.h_val + 4, 8, cudaMemcpyHostToDevice, S.ctl);
+        cudaStreamSynchronize(S.ctl);
+    }
     cudaStreamSynchronize(S.stream);
-    cudaStreamSynchronize(S.ctl);
-    cudaFree(S.d_scratch.ptr);
-    S.d_scratch.ptr = nullptr;
-    cudaFree(S.d_head.ptr);
-    S.d_head.ptr = nullptr;
-    cudaFree(S.d_done.ptr);
-    S.d_done.ptr = nullptr;
-    cudaFreeHost(S.h_jobs);
-    cudaFreeHost(S.h_items[0]);
-    cudaFreeHost(S.h_items[1]);
-    cudaFreeHost(S.h_tail);
+    cudaFree(S.d_scratch);
+    cudaFree(S.d_items[0]);
+    cudaFree(S.d_items[1]);
+    cudaFree(S.d_ctl);
+    cudaFree(S.d_jobs);
+    cudaFree(S.d_done);
+    cudaFreeHost(S.h_stage);
+    cudaFreeHost(S.h_rec);
+    cudaFreeHost(S.h_val);
     cudaFreeHost(S.h_finished);
-    cudaFreeHost(S.h_stop);
     cudaEventDestroy(S.done_ev);
     cudaStreamDestroy(S.stream);
     cudaStreamDestroy(S.ctl);
@@ -3085,15 +3104,20 @@ void PoaService::dispatcher() {
             }
         }
         if (!S.error.empty()) continue;
-        if (S.published[0] + S.published[1] == 0) continue;
-        unsigned long long head[2] = {0, 0};
-        if (cudaMemcpyAsync(head, S.d_head.ptr, 16, cudaMemcpyDeviceToHost, S.ctl) != cudaSuccess ||
-            cudaStreamSynchronize(S.ctl) != cudaSuccess) {
-            S.error = "rb_poa service: head read failed";
-            S.cv_slot.notify_all();
-            continue;
+        bool pending = false;
+        {
+            // lock order: mu, then pub_mu (publishers take pub_mu alone)
+            std::lock_guard<std::mutex> plk(S.pub_mu);
+            if (S.published[0] + S.published[1] == 0) continue;
+            if (cudaMemcpyAsync(S.h_val + 2, S.d_ctl + 2, 16, cudaMemcpyDeviceToHost, S.ctl) != cudaSuccess ||
+                cudaStreamSynchronize(S.ctl) != cudaSuccess) {
+                S.error = "rb_poa service: head read failed";
+                S.cv_slot.notify_all();
+                continue;
+            }
+            pending = S.h_val[2] < S.published[0] || S.h_val[3] < S.published[1];
         }
-        if (head[0] >= S.published[0] && head[1] >= S.published[1]) continue;
+        if (!pending) continue;
         poa_service_kernel<<<S.grid, 32 * kWarpsPerCta, kWarpsPerCta * kRingBytesPerWarp, S.stream>>>(S.args);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaEventRecord(S.done_ev, S.stream);
@@ -3126,23 +3150,34 @@ void PoaService::run_batch(const PoaJobDev& job, const uint32_t* order, size_t n
         S.active_items += n;
         gen = ++S.generation[slot];
     }
-    // the slot's done counter starts from zero before any item is visible
-    check_cuda(cudaMemsetAsync(S.d_done.as<unsigned int>() + slot, 0, 4, S.ctl), "memset done");
-    check_cuda(cudaStreamSynchronize(S.ctl), "service control sync");
     {
-        std::lock_guard<std::mutex> lk(S.mu);
+        // record, items, then tail, in one stream: the slot's done counter
+        // starts from zero and its record is in place before any item is
+        // visible, and the items before the tail
+        std::lock_guard<std::mutex> plk(S.pub_mu);
+        const int q = high_priority ? 0 : 1;
+        const unsigned long long t = S.published[q];
         PoaJobDev rec = job;
         rec.total = uint32_t(n);
         rec.generation = gen;
-        S.h_jobs[slot] = rec;
-        const int q = high_priority ? 0 : 1;
-        uint2* ring = S.h_items[q];
-        unsigned long long t = S.published[q];
-        for (size_t i = 0; i < n; ++i) ring[(t + i) & (kSvcRing - 1)] = make_uint2(slot, order[i]);
+        *S.h_rec = rec;
+        check_cuda(cudaMemsetAsync(S.d_done + slot, 0, 4, S.ctl), "memset done");
+        check_cuda(cudaMemcpyAsync(S.d_jobs + slot, S.h_rec, sizeof(PoaJobDev), cudaMemcpyHostToDevice, S.ctl),
+                   "H2D job record");
+        for (size_t i = 0; i < n; ++i) S.h_stage[i] = make_uint2(slot, order[i]);
+        const size_t at = size_t(t & (kSvcRing - 1));
+        const size_t first = std::min(n, size_t(kSvcRing) - at);
+        check_cuda(cudaMemcpyAsync(S.d_items[q] + at, S.h_stage, first * sizeof(uint2), cudaMemcpyHostToDevice,
+                                   S.ctl),
+                   "H2D items");
+        if (first < n)
+            check_cuda(cudaMemcpyAsync(S.d_items[q], S.h_stage + first, (n - first) * sizeof(uint2),
+                                       cudaMemcpyHostToDevice, S.ctl),
+                       "H2D items");
+        S.h_val[q] = t + n;
+        check_cuda(cudaMemcpyAsync(S.d_ctl + q, S.h_val + q, 8, cudaMemcpyHostToDevice, S.ctl), "H2D tail");
+        check_cuda(cudaStreamSynchronize(S.ctl), "service publish");
         S.published[q] = t + n;
-        std::atomic_thread_fence(std::memory_order_release);
-        reinterpret_cast<volatile unsigned long long*>(S.h_tail)[q] = t + n;
-        std::atomic_thread_fence(std::memory_order_seq_cst);
     }
     S.cv.notify_all();
     // wait for the batch; the dispatcher keeps a kernel running meanwhile
