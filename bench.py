@@ -46,6 +46,11 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # this times its cells
 POA_DRAM_BYTES_PER_CELL = (1.783481e9 + 27.338935e9) / 5838774640
 L2_FLUSH_BYTES = 512 << 20
+# DRAM bytes (read + write) of nw_distance_kernel per nominal cell (query x
+# target span) from one ncu capture of the first 500 pairs of the config-2
+# batch (31.4 MB read + 104.8 MB written over 421.3 G nominal cells); the
+# strip carry buffers grow with the swept cells
+NWD_DRAM_BYTES_PER_CELL = (31.4e6 + 104.8e6) / 421325730898
 
 
 def _args():
@@ -406,7 +411,10 @@ def run_align(args, local, world, rank):
                    "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps},
            "roofline": {"bound": "hbm", "kernel": "nw_distance_kernel + nw_level_kernel",
                         "achieved": achieved_gbs, "peak": peaks.get("hbm_gbs", 6650.0), "unit": "GB/s",
-                        "frac": achieved_gbs / peaks.get("hbm_gbs", 6650.0), "traffic": None,
+                        "frac": achieved_gbs / peaks.get("hbm_gbs", 6650.0),
+                        "traffic": nominal * NWD_DRAM_BYTES_PER_CELL,
+                        "traffic_source": "nw_distance_kernel DRAM bytes per nominal cell from a 500-pair ncu "
+                                          "capture, times this step's nominal cells",
                         "note": "algorithmic bytes = sequences in + CIGAR and breakpoints out; the sweep is "
                                 "integer-issue bound, see compute"},
            "compute": {"bound": "int32 issue", "achieved_tops": achieved_tops, "peak_tops": int_peak_tops,

@@ -224,13 +224,19 @@ __global__ void __launch_bounds__(256) quality_check_kernel(const uint8_t* store
 
 // Exclusive prefix sum of n counts into base (one CTA of 1024 threads, tiles
 // of 4096 with a running carry); base[n] = total.
-__global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* cnt, uint64_t* base, uint32_t n) {
+// One small block: a kernel of this context must fit beside the persistent
+// kernels that other contexts (the serving loop's shared consensus kernel)
+// keep resident, or it would wait for them to drain.
+constexpr int kScanThreads = 256;
+constexpr int kScanWarps = kScanThreads / 32;
+
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(const uint32_t* cnt, uint64_t* base, uint32_t n) {
     __shared__ unsigned long long warp_sum[32];
     __shared__ unsigned long long carry;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (uint32_t t0 = 0; t0 < n; t0 += 4096) {
+    for (uint32_t t0 = 0; t0 < n; t0 += kScanThreads * 4) {
         uint32_t v[4];
         unsigned long long s = 0;
 #pragma unroll
@@ -249,7 +255,7 @@ __global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* cnt, uint64_
         if (lane == 31) warp_sum[wid] = x;
         __syncthreads();
         if (wid == 0) {
-            unsigned long long z = warp_sum[lane];
+            unsigned long long z = lane < kScanWarps ? warp_sum[lane] : 0ull;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 const unsigned long long y = __shfl_up_sync(0xffffffffu, z, d);
@@ -266,7 +272,7 @@ __global__ void __launch_bounds__(1024) scan_kernel(const uint32_t* cnt, uint64_
             run += v[u];
         }
         __syncthreads();
-        if (threadIdx.x == 0) carry += warp_sum[31];
+        if (threadIdx.x == 0) carry += warp_sum[kScanWarps - 1];
         __syncthreads();
     }
     if (threadIdx.x == 0) base[n] = carry;
@@ -675,7 +681,7 @@ void LayerEngine::finish(int tgs, int trim, PoaEngine& poa) {
         check_cuda(cudaGetLastError(), "quality_check_kernel");
         ++stats_.launches;
     }
-    scan_kernel<<<1, 1024, 0, stream_>>>(win_cnt(), win_base(), nw);
+    scan_kernel<<<1, kScanThreads, 0, stream_>>>(win_cnt(), win_base(), nw);
     check_cuda(cudaGetLastError(), "scan_kernel");
     ++stats_.launches;
     // totals and status before the layer-sized buffers

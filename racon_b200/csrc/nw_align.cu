@@ -59,7 +59,8 @@ namespace {
 typedef unsigned long long u64;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarpsPerBlock = 4;
-constexpr int kMaxSym = 32;
+constexpr int kMaxSym = 32;        // symbols whose bit masks fit the shared-memory table
+constexpr int kMaxSymWide = 256;   // any byte alphabet: the masks then live in the warp's scratch
 constexpr long long kLeafBytes = 1024 * 1024;  // edlib's traceback threshold
 
 enum NwStatus : int {
@@ -160,8 +161,13 @@ struct WarpScratch {
     u64* capr_pv;
     u64* capr_mv;
     int32_t* capr_sc;
-    uint4* leaf;
+    uint4* leaf;  // followed by the [kMaxSymWide][32] bit masks of pairs with more than kMaxSym symbols
 };
+
+// Bit masks of a wide-alphabet pair: the region after the leaf store.
+__device__ __forceinline__ u64* peq_wide(const WarpScratch& ws) {
+    return reinterpret_cast<u64*>(reinterpret_cast<uint8_t*>(ws.leaf) + kLeafBytes);
+}
 
 __device__ WarpScratch warp_scratch(const NwDevArgs& a, uint32_t slot) {
     uint8_t* p = a.scratch + size_t(slot) * a.scratch_stride;
@@ -182,13 +188,14 @@ __device__ WarpScratch warp_scratch(const NwDevArgs& a, uint32_t slot) {
     w.capr_pv = reinterpret_cast<u64*>(take(nb * 8));
     w.capr_mv = reinterpret_cast<u64*>(take(nb * 8));
     w.capr_sc = reinterpret_cast<int32_t*>(take(nb * 4));
-    w.leaf = reinterpret_cast<uint4*>(take(kLeafBytes));
+    w.leaf = reinterpret_cast<uint4*>(take(kLeafBytes));  // kLeafBytes is a multiple of 256
     return w;
 }
 
 size_t warp_scratch_bytes(size_t n, size_t nb) {
     auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
-    return 2 * r(n) + 2 * r(n * 4) + 2 * (2 * r(nb * 8) + r(nb * 4)) + r(kLeafBytes);
+    return 2 * r(n) + 2 * r(n * 4) + 2 * (2 * r(nb * 8) + r(nb * 4)) + r(kLeafBytes) +
+           r(size_t(kMaxSymWide) * 32 * 8);
 }
 
 enum SweepMode { kDistance = 0, kCapture = 1, kLeaf = 2 };
@@ -371,7 +378,7 @@ __device__ void leaf_traceback(const NwDevArgs& a, const NwPairDev& P, const NwT
     io.rev = false;
     io.ncols = n;
     io.nsym = int(P.nsym);
-    io.peq = peq;
+    io.peq = int(P.nsym) <= kMaxSym ? peq : peq_wide(ws);
     io.leaf = ws.leaf;
     io.bw = bw;
     warp_sweep<kLeaf>(io, B, ws, lane, a.counters);
@@ -474,7 +481,7 @@ __device__ void hirschberg_split(const NwDevArgs& a, const NwPairDev& P, const N
     io.q = a.codes + P.q_off + T.qa;
     io.t = a.codes + P.t_off + T.ta;
     io.nsym = int(P.nsym);
-    io.peq = peq;
+    io.peq = int(P.nsym) <= kMaxSym ? peq : peq_wide(ws);
     io.leaf = nullptr;
     io.bw = 0;
     io.rev = false;
@@ -601,6 +608,7 @@ nw_distance_kernel(NwDevArgs a) {
         io.ncols = n;
         io.nsym = int(P.nsym);
         io.peq = peq;
+        if (int(P.nsym) > kMaxSym) io.peq = peq_wide(warp_scratch(a, slot));
         io.leaf = nullptr;
         io.bw = 0;
         int k = max(64, abs(m - n));
@@ -829,8 +837,9 @@ __global__ void __launch_bounds__(256) nw_cigar_kernel(NwDevArgs a, uint64_t* le
     }
 }
 
-__global__ void exclusive_scan_kernel(const uint64_t* in, uint64_t* out, uint32_t n) {
-    // single block; n up to a few million
+__global__ void __launch_bounds__(256) exclusive_scan_kernel(const uint64_t* in, uint64_t* out, uint32_t n) {
+    // single block of 256 threads (small enough to fit beside the serving
+    // loop's resident consensus kernel); n up to a few million
     __shared__ uint64_t part[1024];
     const uint32_t tid = threadIdx.x;
     const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
@@ -1037,7 +1046,7 @@ struct NwStoreSrc {
 // NwEngine::stage gives on the host), one warp per pair. First appearances
 // come from one pass over 32-byte chunks in order: the lowest lane holding a
 // byte value not seen before records its position. A pair with more than
-// kMaxSym distinct bytes sets status[0] = 1 and is not encoded.
+// kMaxSymWide distinct bytes (impossible for bytes) sets status[0] = 1.
 __global__ void __launch_bounds__(256) nw_encode_kernel(const uint8_t* store, const NwStoreSrc* src,
                                                         NwPairDev* pairs, uint8_t* codes, uint32_t n,
                                                         unsigned int* status) {
@@ -1074,7 +1083,7 @@ __global__ void __launch_bounds__(256) nw_encode_kernel(const uint8_t* store, co
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) present += __shfl_xor_sync(0xffffffffu, present, d);
         __syncwarp();
-        if (present > kMaxSym) {
+        if (present > kMaxSymWide) {  // cannot happen for byte symbols; kept as a guard
             if (lane == 0) status[0] = 1u;
             continue;
         }
@@ -1218,7 +1227,7 @@ void NwEngine::stage(const rb_pair* pairs, size_t n, int want_cigar, uint32_t wi
     }
     check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
     check_cuda(cudaStreamSynchronize(stream_), "stage sync");
-    if (status) throw Error{RB_ERR_ARG, "rb_align: more than 32 distinct symbols in a pair"};
+    if (status) throw Error{RB_ERR_ARG, "rb_align: symbol coding failed"};
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0_, ev1_);
     stats_.h2d_ms = ms;
@@ -1309,7 +1318,7 @@ void NwEngine::stage_store(const rb_store_pair* pairs, size_t n, int want_cigar,
     unsigned int status = 0;
     if (n) check_cuda(cudaMemcpyAsync(&status, d_misc_.ptr, 4, cudaMemcpyDeviceToHost, stream_), "D2H status");
     check_cuda(cudaStreamSynchronize(stream_), "stage sync");
-    if (status) throw Error{RB_ERR_ARG, "rb_align: more than 32 distinct symbols in a pair"};
+    if (status) throw Error{RB_ERR_ARG, "rb_align: symbol coding failed"};
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0_, ev1_);
     stats_.h2d_ms = ms;
@@ -1416,7 +1425,7 @@ void NwEngine::run() {
         d_cigoff_.reserve((n + 1) * sizeof(uint64_t));
         nw_cigar_kernel<<<warp_grid, 256, 0, stream_>>>(a, d_ciglen_.as<uint64_t>(), nullptr,
                                                                    nullptr, 0);
-        exclusive_scan_kernel<<<1, 1024, 0, stream_>>>(d_ciglen_.as<uint64_t>(), d_cigoff_.as<uint64_t>(),
+        exclusive_scan_kernel<<<1, 256, 0, stream_>>>(d_ciglen_.as<uint64_t>(), d_cigoff_.as<uint64_t>(),
                                                        uint32_t(n));
         uint64_t total = 0;
         check_cuda(cudaMemcpyAsync(&total, d_cigoff_.as<uint64_t>() + n, 8, cudaMemcpyDeviceToHost, stream_),

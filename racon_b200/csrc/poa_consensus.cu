@@ -1104,6 +1104,10 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
 #pragma unroll
     for (int k = 0; k < S; ++k) hv[k] = (j0 + k) * gap;
     int left_prev = lane == 0 ? kNegInf : (j0 - 1) * gap;
+    // the next row's descriptor is read while this row's scan and stores
+    // are in flight (from the staged block, or from `pre` at a block edge)
+    int4 dnext = make_int4(__shfl_sync(kFull, pre.x, 0), __shfl_sync(kFull, pre.y, 0),
+                           __shfl_sync(kFull, pre.z, 0), __shfl_sync(kFull, pre.w, 0));
     for (int i = 1; i <= ndp; ++i) {
         const int bi = (i - 1) & 31;
         if (bi == 0) {
@@ -1113,7 +1117,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
             const int nx = i - 1 + 32 + lane;
             pre = nx < ndp ? rowdesc[nx] : make_int4(0, 0, 0, 0);
         }
-        const int4 d = dblk[bi];
+        const int4 d = dnext;
         const int np = desc_np(d.w);
         npreds += np;
         const bool is_sink = desc_sink(d.w);
@@ -1129,14 +1133,23 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
             if (r == 0) {
 #pragma unroll
                 for (int k = 0; k < S; ++k) hv[k] = (j0 + k) * gap;
-            } else {
-                const bool in_ring = i - r <= R;
-                const int4* src = in_ring ? ring + (r % R) * Q * 32 + lane
-                                          : reinterpret_cast<const int4*>(Hm + r * lc + j0);
-                const int stride = in_ring ? 32 : 1;
+            } else if (i - r <= R) {
+                // separate shared and global paths (warp-uniform branch), so
+                // the ring is read with shared-memory loads, not generic ones
+                const int4* src = ring + (r % R) * Q * 32 + lane;
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
-                    const int4 t4 = src[q * stride];
+                    const int4 t4 = src[q * 32];
+                    hv[4 * q] = t4.x;
+                    hv[4 * q + 1] = t4.y;
+                    hv[4 * q + 2] = t4.z;
+                    hv[4 * q + 3] = t4.w;
+                }
+            } else {
+                const int4* src = reinterpret_cast<const int4*>(Hm + r * lc + j0);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const int4 t4 = src[q];
                     hv[4 * q] = t4.x;
                     hv[4 * q + 1] = t4.y;
                     hv[4 * q + 2] = t4.z;
@@ -1213,6 +1226,15 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         int cin = __shfl_up_sync(kFull, x, 1);  // final value left of the segment
         if (lane == 0) cin = kNegInf;
         left_prev = cin;
+        if (i < ndp) {
+            const int bn = i & 31;  // slot of row i + 1 in the staged block
+            if (bn == 0) {
+                dnext = make_int4(__shfl_sync(kFull, pre.x, 0), __shfl_sync(kFull, pre.y, 0),
+                                  __shfl_sync(kFull, pre.z, 0), __shfl_sync(kFull, pre.w, 0));
+            } else {
+                dnext = dblk[bn];
+            }
+        }
         uint32_t hq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {

@@ -131,6 +131,24 @@ def test_config2_batch_sample(ctx, oracle_lib):
     _check_parallel(ctx, oracle_lib, synthetic.pairs(1000, 1_000, 50_000, seed=22), 500)
 
 
+def test_wide_alphabet(ctx, oracle_lib):
+    # more than 32 distinct bytes in a pair (IUPAC codes, lowercase, other
+    # printable bytes): edlib aligns any byte alphabet, and so must the device
+    # (its query masks then live in global scratch instead of shared memory)
+    rng = random.Random(11)
+    iupac = "ACGTURYKMSWBDHVN"
+    wide = iupac + "acgturykmswbdhvn" + "0123456789!#$%&*+-.:;<=>?@"
+    pairs = []
+    for i, (lo, hi) in enumerate([(1, 80), (200, 2000), (6000, 9000)] * 4):
+        alpha = wide if i % 3 else iupac + "xyz*-"
+        n = rng.randint(lo, hi)
+        t = "".join(rng.choice(alpha) for _ in range(n))
+        q = _mutate(rng, t, 0.06, 0.03, 0.03, alpha) or "A"
+        pairs.append({"query": q, "target": t, "q_offset": rng.randint(0, 500), "t_begin": rng.randint(0, 2000)})
+    assert any(len(set(p["query"] + p["target"])) > 32 for p in pairs)
+    _check(ctx, oracle_lib, pairs, 500)
+
+
 def test_stage_run_fetch_matches_batch(ctx, oracle_lib):
     pairs = _random_pairs(5, 50, 100, 2000, 0.12)
     a = ctx.align(pairs, want_cigar=True)
