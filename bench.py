@@ -68,7 +68,7 @@ def _args():
     p.add_argument("--data-dir", default=None)
     p.add_argument("--serving-jobs", type=int, default=12, help="config-4 jobs in the serving measurement "
                    "(0 = skip it)")
-    p.add_argument("--workers", type=int, default=4, help="serving-loop workers")
+    p.add_argument("--workers", type=int, default=8, help="serving-loop workers")
     p.add_argument("--pairs", type=int, default=10000, help="config-2 pairs per step")
     return p.parse_args()
 

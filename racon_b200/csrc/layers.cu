@@ -348,6 +348,12 @@ uint64_t align16(uint64_t x) { return (x + 15) & ~uint64_t(15); }
 LayerEngine::LayerEngine(const DeviceInfo& dev, cudaStream_t stream) : dev_(dev), stream_(stream) {
     check_cuda(cudaEventCreate(&ev0_), "cudaEventCreate");
     check_cuda(cudaEventCreate(&ev1_), "cudaEventCreate");
+    const void* kernels[] = {reinterpret_cast<const void*>(revcomp_kernel),
+                             reinterpret_cast<const void*>(layer_candidates_kernel),
+                             reinterpret_cast<const void*>(quality_check_kernel),
+                             reinterpret_cast<const void*>(scan_kernel), reinterpret_cast<const void*>(place_kernel),
+                             reinterpret_cast<const void*>(order_kernel), reinterpret_cast<const void*>(gather_kernel)};
+    for (const void* k : kernels) prefer_max_shared(k);
 }
 
 LayerEngine::~LayerEngine() {

@@ -1107,6 +1107,15 @@ NwEngine::NwEngine(const DeviceInfo& dev, cudaStream_t stream) : dev_(dev), stre
     check_cuda(cudaFuncSetAttribute(nw_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     kWarpsPerBlock * kMaxSym * 32 * 8),
                "cudaFuncSetAttribute");
+    const void* kernels[] = {reinterpret_cast<const void*>(nw_distance_kernel),
+                             reinterpret_cast<const void*>(nw_root_tasks_kernel),
+                             reinterpret_cast<const void*>(nw_level_kernel),
+                             reinterpret_cast<const void*>(nw_breakpoints_kernel),
+                             reinterpret_cast<const void*>(nw_cigar_kernel),
+                             reinterpret_cast<const void*>(exclusive_scan_kernel),
+                             reinterpret_cast<const void*>(cigar_breakpoints_kernel),
+                             reinterpret_cast<const void*>(nw_encode_kernel)};
+    for (const void* k : kernels) prefer_max_shared(k);
 }
 
 NwEngine::~NwEngine() {

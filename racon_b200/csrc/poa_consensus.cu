@@ -2562,6 +2562,8 @@ PoaEngine::PoaEngine(const DeviceInfo& dev, cudaStream_t stream, int8_t m, int8_
     check_cuda(cudaEventCreate(&ev1_), "cudaEventCreate");
     check_cuda(cudaEventCreate(&ev2_), "cudaEventCreate");
     check_cuda(cudaEventCreate(&ev3_), "cudaEventCreate");
+    prefer_max_shared(reinterpret_cast<const void*>(poa_kernel));
+    prefer_max_shared(reinterpret_cast<const void*>(poa_plain_kernel));
 }
 
 PoaEngine::~PoaEngine() {
@@ -3065,6 +3067,8 @@ PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window
     check_cuda(cudaFuncSetAttribute(poa_service_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     kWarpsPerCta * kRingBytesPerWarp),
                "cudaFuncSetAttribute");
+    prefer_max_shared(reinterpret_cast<const void*>(poa_service_kernel));
+    keep_pool_reserve(device);
     S.thread = std::thread([this] { dispatcher(); });
 }
 

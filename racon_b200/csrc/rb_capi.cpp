@@ -61,16 +61,36 @@ void DevBuf::release() {
 }
 void HostBuf::reserve(size_t need) {
     if (need <= bytes && ptr) return;
-    release();
+    // the outgrown buffer is kept until the owner is destroyed: cudaFreeHost
+    // synchronises the whole device, which with a resident persistent kernel
+    // of another context (the serving loop) would wait for that kernel
+    if (ptr) retired.push_back(ptr);
+    ptr = nullptr;
+    bytes = 0;
     size_t b = need < 256 ? 256 : need;
-    b = b + b / 4;  // headroom for growing batches
+    b = b + b / 2;  // headroom for growing batches (few growth steps)
     check_cuda(cudaMallocHost(&ptr, b), "cudaMallocHost");
     bytes = b;
 }
 void HostBuf::release() {
     if (ptr) cudaFreeHost(ptr);
+    for (void* r : retired) cudaFreeHost(r);
+    retired.clear();
     ptr = nullptr;
     bytes = 0;
+}
+
+void prefer_max_shared(const void* kernel) {
+    check_cuda(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    int(cudaSharedmemCarveoutMaxShared)),
+               "cudaFuncSetAttribute carveout");
+}
+
+void keep_pool_reserve(int device) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return;
+    uint64_t keep = ~uint64_t(0);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
 }
 
 namespace {
@@ -214,6 +234,7 @@ rb_ctx* rb_create(int device, const rb_params* params) {
         rb::check_cuda(cudaStreamCreateWithPriority(&ctx->stream_hi, cudaStreamNonBlocking, greatest),
                        "cudaStreamCreateWithPriority");
         ctx->stream = ctx->stream_lo;
+        rb::keep_pool_reserve(device);
         ctx->nw.reset(new rb::NwEngine(ctx->dev, ctx->stream));
         ctx->poa.reset(new rb::PoaEngine(ctx->dev, ctx->stream, params->match, params->mismatch, params->gap));
         ctx->layers.reset(new rb::LayerEngine(ctx->dev, ctx->stream));

@@ -35,10 +35,11 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
-// Growable pinned host buffer.
+// Growable pinned host buffer (outgrown buffers are freed with it).
 struct HostBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    std::vector<void*> retired;
     void reserve(size_t need);
     void release();
     template <class T> T* as() const { return static_cast<T*>(ptr); }
@@ -59,6 +60,17 @@ struct DeviceInfo {
     int sm_count = 148;
     size_t smem_optin = 0;
 };
+
+// Every kernel of the library asks for the largest shared-memory carveout, so
+// an SM never has to change its L1/shared split between kernels. A change
+// can only happen on an idle SM, so kernels of one context would otherwise
+// wait for another context's resident persistent kernel (the serving loop's
+// shared consensus kernel) to drain.
+void prefer_max_shared(const void* kernel);
+// The device's default memory pool keeps what it has reserved: trimming it
+// at synchronisation points can wait for the device (and so for a resident
+// persistent kernel). Called once per device when a context is created.
+void keep_pool_reserve(int device);
 
 // Launch choices of a device (rb_tuning), read by the engines at every run.
 rb_tuning tuning_get(int device);
