@@ -69,6 +69,8 @@ def _args():
     p.add_argument("--serving-jobs", type=int, default=12, help="config-4 jobs in the serving measurement "
                    "(0 = skip it)")
     p.add_argument("--workers", type=int, default=8, help="serving-loop workers")
+    p.add_argument("--no-shared-consensus", action="store_true",
+                   help="serving: each job launches its own consensus kernel")
     p.add_argument("--pairs", type=int, default=10000, help="config-2 pairs per step")
     return p.parse_args()
 
@@ -214,7 +216,9 @@ def _serving_jobs(args):
     if os.path.exists(marker):
         with open(marker) as fh:
             return json.load(fh)
+    t0 = time.perf_counter()
     jobs = synthetic.serving_jobs(d, args.serving_jobs, seed=4)
+    sys.stderr.write("[serving] generated %d jobs in %.1f s\n" % (len(jobs), time.perf_counter() - t0))
     with open(marker, "w") as fh:
         json.dump(jobs, fh)
     return jobs
@@ -246,8 +250,15 @@ def run_serving(args, device, rates):
     free_b, _ = torch.cuda.mem_get_info(device)
     budget = int(free_b * 0.7)
     out["hbm_budget"] = budget
+    out["shared_consensus"] = not args.no_shared_consensus
+    t_start = time.perf_counter()
+
+    def log(msg):
+        sys.stderr.write("[serving %.1fs] %s\n" % (time.perf_counter() - t_start, msg))
+        sys.stderr.flush()
+
     with racon_b200.Server(device, workers=args.workers, hbm_budget=budget, match=3, mismatch=-5, gap=-4,
-                           window_length=w) as srv:
+                           window_length=w, shared_consensus=not args.no_shared_consensus) as srv:
         def run(arrivals):
             t0 = time.perf_counter()
             tickets = []
@@ -261,20 +272,25 @@ def run_serving(args, device, rates):
             span = max(r[1]["finished"] for r in res) - min(r[1]["submitted"] for r in res)
             return [r[0] for r in res], [r[1] for r in res], span
 
+        log("server up, %d jobs, %d windows" % (len(jobs), sum(windows)))
         run(None)  # warm-up pass
+        log("warm-up pass done")
         # every worker's buffers at the working size: the largest job once per
         # worker, all at once (an idle worker takes each)
         big = max(range(len(jobs)), key=lambda i: windows[i])
         for t in [srv.submit(*jobs[big][:3]) for _ in range(args.workers)]:
             srv.wait(t)
+        log("workers warmed with the largest job")
         iso, alone = [], []
         for j in jobs:
             fasta, tm = srv.wait(srv.submit(j[0], j[1], j[2]))
             alone.append(fasta)
             iso.append(tm["finished"] - tm["submitted"])
+        log("isolated runs done, sum %.2f s" % sum(iso))
         fastas, _, span = run(None)
         assert fastas == alone, "a job's output differs between alone and in the mix"
         peak = len(jobs) / span
+        log("peak run done, makespan %.2f s" % span)
         out.update(isolated_s={"p50": _pct(iso, 50), "max": max(iso), "sum": sum(iso)},
                    peak={"jobs_per_s": peak, "windows_per_s": sum(windows) / span, "makespan_s": span})
         sweep = []
@@ -289,9 +305,17 @@ def run_serving(args, device, rates):
             assert fastas == alone, "a job's output differs between alone and in the mix"
             lat = [tm["finished"] - tm["submitted"] for tm in times]
             ratio = [a / b for a, b in zip(lat, iso)]
+            # where a job's time went: queueing for a worker, then the job's
+            # stages on it (load, alignment + layers, window records, consensus)
+            wait = [tm["admitted"] - tm["submitted"] for tm in times]
+            stages = [[tm["stage_seconds"][k] for tm in times] for k in range(4)]
+            log("load %.2f done, makespan %.2f s, p99 latency %.2f s" % (frac, span, _pct(lat, 99)))
             sweep.append({"load": frac, "jobs_per_s": len(jobs) / span, "windows_per_s": sum(windows) / span,
                           "latency_s": {"p50": _pct(lat, 50), "p99": _pct(lat, 99)},
-                          "latency_vs_isolated": {"p50": _pct(ratio, 50), "p99": _pct(ratio, 99)}})
+                          "latency_vs_isolated": {"p50": _pct(ratio, 50), "p99": _pct(ratio, 99)},
+                          "admission_wait_s": {"mean": sum(wait) / len(wait), "max": max(wait)},
+                          "stage_mean_s": [sum(x) / len(x) for x in stages],
+                          "stage_max_s": [max(x) for x in stages]})
         out["rates"] = sweep
     return out
 
