@@ -2454,6 +2454,7 @@ struct PoaSvcArgs {
     const uint2* items[2];           // device rings: (job slot, window), [0] = high priority
     const unsigned long long* tail;  // device: [2] items published
     unsigned long long* head;        // device: [2] items claimed
+    unsigned int* live;              // device: [0] warps working on a window, [1] closing (per launch)
     unsigned long long ring_mask;
     unsigned int* done;              // device: windows finished per job slot
     volatile unsigned int* finished; // mapped host: generation of the last finished batch per slot
@@ -2462,23 +2463,29 @@ struct PoaSvcArgs {
 };
 
 // Claims the next item, high-priority ring first: returns (job << 32) |
-// window, or ~0 after idle_ns without work or when stop is set (bounded: the
-// kernel always ends). Out of line with scalar arguments, so its registers
-// do not add to the window code's.
+// window, or ~0 when the kernel closes or stop is set. The kernel closes as a
+// whole: a warp that has found no work for idle_ns while no warp of the
+// kernel is working sets the closing word, and every warp leaves at its next
+// poll. (Warps that left one by one would leave work arriving later to the
+// few still busy.) Bounded: once no window is in flight, the kernel ends
+// within idle_ns plus one poll. Out of line with scalar arguments, so its
+// registers do not add to the window code's.
 __device__ __noinline__ unsigned long long svc_claim(const uint2* items0, const uint2* items1,
                                                      const unsigned long long* tail, unsigned long long* head,
-                                                     unsigned long long ring_mask, const unsigned int* stop,
-                                                     unsigned long long idle_ns) {
+                                                     unsigned int* live, unsigned long long ring_mask,
+                                                     const unsigned int* stop, unsigned long long idle_ns) {
     const unsigned long long t0 = global_ns();
     unsigned int nap = 512;
+    volatile unsigned int* vlive = live;
     for (;;) {
-        if (*reinterpret_cast<const volatile unsigned int*>(stop)) return ~0ull;
+        if (*reinterpret_cast<const volatile unsigned int*>(stop) || vlive[1]) return ~0ull;
         for (int q = 0; q < 2; ++q) {
             const unsigned long long t = reinterpret_cast<const volatile unsigned long long*>(tail)[q];
             unsigned long long h = reinterpret_cast<volatile unsigned long long*>(head)[q];
             while (h < t) {
                 const unsigned long long prev = atomicCAS(head + q, h, h + 1);
                 if (prev == h) {
+                    atomicAdd(live, 1u);
                     __threadfence();
                     const volatile unsigned int* it =
                         reinterpret_cast<const volatile unsigned int*>((q ? items1 : items0) + (h & ring_mask));
@@ -2487,7 +2494,10 @@ __device__ __noinline__ unsigned long long svc_claim(const uint2* items0, const 
                 h = prev;
             }
         }
-        if (global_ns() - t0 > idle_ns) return ~0ull;
+        if (global_ns() - t0 > idle_ns && vlive[0] == 0) {
+            atomicExch(live + 1, 1u);
+            return ~0ull;
+        }
         __nanosleep(nap);
         nap = nap < 32768 ? nap * 2 : nap;
     }
@@ -2512,7 +2522,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
     for (;;) {
         unsigned long long it = 0;
         if (lane == 0)
-            it = svc_claim(s.items[0], s.items[1], s.tail, s.head, s.ring_mask, s.stop, s.idle_ns);
+            it = svc_claim(s.items[0], s.items[1], s.tail, s.head, s.live, s.ring_mask, s.stop, s.idle_ns);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it == ~0ull) break;
         const uint32_t job = uint32_t(it >> 32), win = uint32_t(it);
@@ -2545,6 +2555,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
                 __threadfence_system();
                 s.finished[job] = gen;
             }
+            atomicSub(s.live, 1u);
         }
     }
 }
@@ -3058,6 +3069,7 @@ PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window
     A.tail = S.d_ctl;
     A.head = S.d_ctl + 2;
     A.stop = reinterpret_cast<const unsigned int*>(S.d_ctl + 4);
+    A.live = reinterpret_cast<unsigned int*>(S.d_ctl + 6);
     A.ring_mask = kSvcRing - 1;
     A.done = S.d_done;
     A.finished = static_cast<unsigned int*>(d_fin);
@@ -3144,8 +3156,11 @@ void PoaService::dispatcher() {
             pending = S.h_val[2] < S.published[0] || S.h_val[3] < S.published[1];
         }
         if (!pending) continue;
-        poa_service_kernel<<<S.grid, 32 * kWarpsPerCta, kWarpsPerCta * kRingBytesPerWarp, S.stream>>>(S.args);
-        cudaError_t e = cudaGetLastError();
+        // a launch starts with no warp working and not closing
+        cudaError_t e = cudaMemsetAsync(S.d_ctl + 6, 0, 8, S.stream);
+        if (e == cudaSuccess)
+            poa_service_kernel<<<S.grid, 32 * kWarpsPerCta, kWarpsPerCta * kRingBytesPerWarp, S.stream>>>(S.args);
+        if (e == cudaSuccess) e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaEventRecord(S.done_ev, S.stream);
         if (e != cudaSuccess) {
             S.error = std::string("rb_poa service launch: ") + cudaGetErrorString(e);
