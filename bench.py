@@ -17,11 +17,19 @@ untimed; a step is the consensus of every window of the job.
   e2e_host_layers  the same through rb_poa_batch with host-assembled
          windows (pack every layer's bases, H2D, kernels, D2H, unpack)
   roofline / compute  HBM bytes (bases and qualities in, consensus out) and
-         int32 issue (about 6 ops per DP cell) of poa_kernel; the POA DP is
+         int32 issue of poa_kernel from the edge-cells the kernel counts
+         (|layer| x sum_v (1 + in-degree v), 3 int ops each); the POA DP is
          integer-issue bound
+  tuning  the launch choices rb_autotune measured on this job
+  parity  the oracle's consensus of the CPU sample against the device's,
+         window by window
   cpu_baseline  the CPU oracle (restatement of racon's algorithm, not
          reference racon, which does not build here) on a bounded sample of
          the same windows with every host thread
+  pipeline  the whole job through rb_polish_files against the oracle's
+         pipeline on every host thread, FASTA compared byte for byte
+  serving  config-4 jobs through the serving loop (shared consensus kernel)
+         at 80 % of its measured peak
 
 --impl reference runs the CPU oracle as the reference arm (rank 0 only).
 Multi-GPU: one process per GPU (torchrun); each rank polishes its own job
