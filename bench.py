@@ -79,6 +79,8 @@ def _args():
     p.add_argument("--workers", type=int, default=8, help="serving-loop workers")
     p.add_argument("--no-shared-consensus", action="store_true",
                    help="serving: each job launches its own consensus kernel")
+    p.add_argument("--alignment-yield", type=int, default=0,
+                   help="serving: alignment pairs per warp and launch for large jobs (0: persistent)")
     p.add_argument("--pairs", type=int, default=10000, help="config-2 pairs per step")
     return p.parse_args()
 
@@ -259,6 +261,7 @@ def run_serving(args, device, rates):
     budget = int(free_b * 0.7)
     out["hbm_budget"] = budget
     out["shared_consensus"] = not args.no_shared_consensus
+    out["alignment_yield"] = args.alignment_yield
     t_start = time.perf_counter()
 
     def log(msg):
@@ -266,7 +269,8 @@ def run_serving(args, device, rates):
         sys.stderr.flush()
 
     with racon_b200.Server(device, workers=args.workers, hbm_budget=budget, match=3, mismatch=-5, gap=-4,
-                           window_length=w, shared_consensus=not args.no_shared_consensus) as srv:
+                           window_length=w, shared_consensus=not args.no_shared_consensus,
+                           alignment_yield=args.alignment_yield) as srv:
         def run(arrivals):
             t0 = time.perf_counter()
             tickets = []

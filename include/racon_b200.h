@@ -387,7 +387,11 @@ void rb_free(void* p);
  * consensus_ctas_per_sm (0 or more than 2: 2) sizes that kernel; the rest of each
  * SM stays free for the alignment and layer kernels of newly admitted jobs.
  * shared_consensus = 0 turns the shared kernel off (each job then launches
- * its own consensus kernel, with its scratch capped at hbm_budget / workers). */
+ * its own consensus kernel, with its scratch capped at hbm_budget / workers).
+ * alignment_yield > 0 puts jobs of at most priority_windows windows on the
+ * high-priority stream and bounds the alignment work of larger jobs to that
+ * many pairs per warp and launch, so that a small job's alignment kernels
+ * find free SMs between a large job's launches (results unchanged). */
 typedef struct rb_server_params {
     int device;
     uint32_t workers;
@@ -399,6 +403,7 @@ typedef struct rb_server_params {
     int shared_consensus;
     uint32_t consensus_ctas_per_sm;
     uint32_t priority_windows;
+    uint32_t alignment_yield;
 } rb_server_params;
 
 /* One job: racon's inputs and per-job flags (-f, -q, -e, --no-trimming, -u). */

@@ -92,7 +92,8 @@ class _ServerParams(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
                 ("match", ctypes.c_int8), ("mismatch", ctypes.c_int8), ("gap", ctypes.c_int8),
                 ("window_length", ctypes.c_uint32), ("shared_consensus", ctypes.c_int),
-                ("consensus_ctas_per_sm", ctypes.c_uint32), ("priority_windows", ctypes.c_uint32)]
+                ("consensus_ctas_per_sm", ctypes.c_uint32), ("priority_windows", ctypes.c_uint32),
+                ("alignment_yield", ctypes.c_uint32)]
 
 
 class _ServerJob(ctypes.Structure):
@@ -629,10 +630,10 @@ class Server:
     first. submit() returns a ticket; wait(ticket) returns (fasta, times)."""
 
     def __init__(self, device=0, workers=4, hbm_budget=0, match=3, mismatch=-5, gap=-4, window_length=500,
-                 shared_consensus=True, consensus_ctas_per_sm=0, priority_windows=0):
+                 shared_consensus=True, consensus_ctas_per_sm=0, priority_windows=0, alignment_yield=0):
         self.lib = load()
         p = _ServerParams(device, workers, hbm_budget, match, mismatch, gap, window_length, int(shared_consensus),
-                          consensus_ctas_per_sm, priority_windows)
+                          consensus_ctas_per_sm, priority_windows, alignment_yield)
         self.ptr = self.lib.rb_server_create(ctypes.byref(p))
         if not self.ptr:
             msg = self.lib.rb_server_error().decode() or self.lib.rb_create_error().decode()

@@ -48,6 +48,7 @@ struct Request {
     std::string sp, op, tp;
     rb_server_job spec{};
     uint64_t footprint = 0;
+    uint64_t windows = 0;  // estimated from the target file size
     double t_submit = 0, t_admit = 0, t_done = 0;
     double stage[4] = {0, 0, 0, 0};
     uint32_t worker = 0;
@@ -127,6 +128,14 @@ struct rb_server {
             std::string fasta, error;
             double stage[4] = {0, 0, 0, 0};
             const rb_server_job& j = r->spec;
+            if (params.alignment_yield) {
+                // small jobs on the high-priority stream with persistent
+                // alignment kernels; large jobs give the SMs back between
+                // bounded launches
+                const bool small = r->windows <= params.priority_windows;
+                rb_set_priority(ctxs[w], small ? 1 : 0);
+                rb_set_yield(ctxs[w], 0, small ? 0u : params.alignment_yield);
+            }
             const int rc = racon::polish_job_on_context(
                 ctxs[w], params.device, r->sp, r->op, r->tp, j.fragment != 0, params.window_length,
                 j.quality_threshold, j.error_threshold, j.trim != 0, params.match, params.mismatch, params.gap,
@@ -177,6 +186,7 @@ rb_server* rb_server_create(const rb_server_params* params) {
     }
     s->poa_cap = s->params.hbm_budget / s->params.workers;
     for (rb_ctx* c : s->ctxs) rb::ctx_set_poa_budget(c, s->poa_cap);
+    if (s->params.priority_windows == 0) s->params.priority_windows = uint32_t(s->sm_count) * 4;
     if (s->params.shared_consensus) {
         // the shared kernel's scratch comes out of the budget once; each
         // worker keeps a small private budget for windows that outgrow it
@@ -189,7 +199,7 @@ rb_server* rb_server_create(const rb_server_params* params) {
             t_server_error = e.msg;
             return nullptr;
         }
-        const uint32_t prio = s->params.priority_windows ? s->params.priority_windows : s->svc->slots() / 4;
+        const uint32_t prio = params->priority_windows ? params->priority_windows : s->svc->slots() / 4;
         s->params.priority_windows = prio;
         for (rb_ctx* c : s->ctxs) {
             rb::ctx_set_poa_budget(c, s->params.hbm_budget / 2 / s->params.workers);
@@ -214,6 +224,7 @@ int rb_server_submit(rb_server* s, const rb_server_job* job, uint64_t* ticket) {
     r->spec.overlaps_path = r->op.c_str();
     r->spec.target_path = r->tp.c_str();
     r->footprint = s->estimate(*r);
+    r->windows = file_bytes(r->tp) / std::max<uint32_t>(1, s->params.window_length) + 1;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->closing || s->stop) {
