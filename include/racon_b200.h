@@ -381,9 +381,10 @@ void rb_free(void* p);
  * Window consensus is continuously batched: one persistent consensus kernel
  * per server takes windows of every job in flight from a shared device work
  * queue, so a job admitted while others run starts on the first free warps
- * instead of waiting for their launches to drain. Jobs of at most
- * priority_windows windows (0: a quarter of the kernel's resident windows)
- * go to a high-priority queue that the kernel drains first.
+ * instead of waiting for their launches to drain. The queue has four rings
+ * by job size, drained smallest first: up to priority_windows windows (0: a
+ * quarter of the kernel's resident windows), up to 4x and 16x that, and
+ * larger.
  * consensus_ctas_per_sm (0 or more than 2: 2) sizes that kernel; the rest of each
  * SM stays free for the alignment and layer kernels of newly admitted jobs.
  * shared_consensus = 0 turns the shared kernel off (each job then launches

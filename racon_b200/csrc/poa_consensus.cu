@@ -2442,6 +2442,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+// Priority rings of the shared queue, drained in order: batches go to ring
+// q by size (ring 0 the smallest), so short jobs start first.
+constexpr int kSvcQueues = 4;
+
 // Queue state lives in device memory: the host writes job records, then
 // items, then the tail with copies in one stream (each copy starts after the
 // previous one completes), so a warp that sees the new tail in L2 finds the
@@ -2451,9 +2455,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
 struct PoaSvcArgs {
     PoaArgs base;                    // scoring, capacities, scratch slots
     const PoaJobDev* jobs;           // device: job records
-    const uint2* items[2];           // device rings: (job slot, window), [0] = high priority
-    const unsigned long long* tail;  // device: [2] items published
-    unsigned long long* head;        // device: [2] items claimed
+    const uint2* items;              // device rings, kSvcQueues x ring_mask + 1 (job slot, window); ring 0 first
+    const unsigned long long* tail;  // device: [kSvcQueues] items published
+    unsigned long long* head;        // device: [kSvcQueues] items claimed
     unsigned int* live;              // device: [0] warps working on a window, [1] closing (per launch)
     unsigned long long ring_mask;
     unsigned int* done;              // device: windows finished per job slot
@@ -2470,7 +2474,7 @@ struct PoaSvcArgs {
 // few still busy.) Bounded: once no window is in flight, the kernel ends
 // within idle_ns plus one poll. Out of line with scalar arguments, so its
 // registers do not add to the window code's.
-__device__ __noinline__ unsigned long long svc_claim(const uint2* items0, const uint2* items1,
+__device__ __noinline__ unsigned long long svc_claim(const uint2* items,
                                                      const unsigned long long* tail, unsigned long long* head,
                                                      unsigned int* live, unsigned long long ring_mask,
                                                      const unsigned int* stop, unsigned long long idle_ns) {
@@ -2479,7 +2483,7 @@ __device__ __noinline__ unsigned long long svc_claim(const uint2* items0, const 
     volatile unsigned int* vlive = live;
     for (;;) {
         if (*reinterpret_cast<const volatile unsigned int*>(stop) || vlive[1]) return ~0ull;
-        for (int q = 0; q < 2; ++q) {
+        for (int q = 0; q < kSvcQueues; ++q) {
             const unsigned long long t = reinterpret_cast<const volatile unsigned long long*>(tail)[q];
             unsigned long long h = reinterpret_cast<volatile unsigned long long*>(head)[q];
             while (h < t) {
@@ -2487,8 +2491,8 @@ __device__ __noinline__ unsigned long long svc_claim(const uint2* items0, const 
                 if (prev == h) {
                     atomicAdd(live, 1u);
                     __threadfence();
-                    const volatile unsigned int* it =
-                        reinterpret_cast<const volatile unsigned int*>((q ? items1 : items0) + (h & ring_mask));
+                    const volatile unsigned int* it = reinterpret_cast<const volatile unsigned int*>(
+                        items + size_t(q) * (ring_mask + 1) + (h & ring_mask));
                     return (static_cast<unsigned long long>(it[0]) << 32) | it[1];
                 }
                 h = prev;
@@ -2522,7 +2526,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
     for (;;) {
         unsigned long long it = 0;
         if (lane == 0)
-            it = svc_claim(s.items[0], s.items[1], s.tail, s.head, s.live, s.ring_mask, s.stop, s.idle_ns);
+            it = svc_claim(s.items, s.tail, s.head, s.live, s.ring_mask, s.stop, s.idle_ns);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it == ~0ull) break;
         const uint32_t job = uint32_t(it >> 32), win = uint32_t(it);
@@ -2978,7 +2982,10 @@ namespace rb {
 
 namespace {
 constexpr uint32_t kSvcJobs = 256;                  // concurrent batches
-constexpr unsigned long long kSvcRing = 1ull << 21; // items per priority ring
+constexpr unsigned long long kSvcRing = 1ull << 21; // items per ring
+// control words (8-byte units): tails, heads, stop, live/closing
+constexpr int kCtlTail = 0, kCtlHead = kSvcQueues, kCtlStop = 2 * kSvcQueues, kCtlLive = 2 * kSvcQueues + 1;
+constexpr size_t kCtlBytes = 128;
 }  // namespace
 
 struct PoaSvcState {
@@ -2991,7 +2998,7 @@ struct PoaSvcState {
     // device: scratch slots, queue rings, [tail0, tail1, head0, head1, stop],
     // job records, per-job done counters
     void* d_scratch = nullptr;
-    uint2* d_items[2] = {nullptr, nullptr};
+    uint2* d_items = nullptr;  // kSvcQueues rings of kSvcRing items
     unsigned long long* d_ctl = nullptr;
     PoaJobDev* d_jobs = nullptr;
     unsigned int* d_done = nullptr;
@@ -3006,7 +3013,7 @@ struct PoaSvcState {
     std::condition_variable cv, cv_slot;
     std::vector<uint32_t> free_jobs;
     std::vector<uint32_t> generation;
-    unsigned long long published[2] = {0, 0};
+    unsigned long long published[kSvcQueues] = {0, 0, 0, 0};
     unsigned long long active_items = 0;
     bool running = false, stopping = false;
     std::string error;
@@ -3036,17 +3043,16 @@ PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window
     S.slots = uint32_t(slots);
     S.grid = uint32_t(slots / kWarpsPerCta);
     check_cuda(cudaMalloc(&S.d_scratch, slots * slot), "cudaMalloc service scratch");
-    check_cuda(cudaMalloc(&S.d_items[0], sizeof(uint2) * kSvcRing), "cudaMalloc service queue");
-    check_cuda(cudaMalloc(&S.d_items[1], sizeof(uint2) * kSvcRing), "cudaMalloc service queue");
-    check_cuda(cudaMalloc(&S.d_ctl, 64), "cudaMalloc");
+    check_cuda(cudaMalloc(&S.d_items, sizeof(uint2) * kSvcRing * kSvcQueues), "cudaMalloc service queue");
+    check_cuda(cudaMalloc(&S.d_ctl, kCtlBytes), "cudaMalloc");
     check_cuda(cudaMalloc(&S.d_jobs, sizeof(PoaJobDev) * kSvcJobs), "cudaMalloc");
     check_cuda(cudaMalloc(&S.d_done, kSvcJobs * 4), "cudaMalloc");
-    check_cuda(cudaMemset(S.d_ctl, 0, 64), "cudaMemset");
+    check_cuda(cudaMemset(S.d_ctl, 0, kCtlBytes), "cudaMemset");
     check_cuda(cudaMemset(S.d_done, 0, kSvcJobs * 4), "cudaMemset");
     check_cuda(cudaMemset(S.d_jobs, 0, sizeof(PoaJobDev) * kSvcJobs), "cudaMemset");
     check_cuda(cudaMallocHost(&S.h_stage, sizeof(uint2) * (kSvcRing / 2)), "cudaMallocHost");
     check_cuda(cudaMallocHost(&S.h_rec, sizeof(PoaJobDev)), "cudaMallocHost");
-    check_cuda(cudaMallocHost(&S.h_val, 64), "cudaMallocHost");
+    check_cuda(cudaMallocHost(&S.h_val, kCtlBytes), "cudaMallocHost");
     check_cuda(cudaHostAlloc(&S.h_finished, 4 * kSvcJobs, cudaHostAllocMapped | cudaHostAllocPortable),
                "cudaHostAlloc mapped");
     memset(S.h_finished, 0, 4 * kSvcJobs);
@@ -3064,12 +3070,11 @@ PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window
     A.base.mismatch = x;
     A.base.gap = g;
     A.jobs = S.d_jobs;
-    A.items[0] = S.d_items[0];
-    A.items[1] = S.d_items[1];
-    A.tail = S.d_ctl;
-    A.head = S.d_ctl + 2;
-    A.stop = reinterpret_cast<const unsigned int*>(S.d_ctl + 4);
-    A.live = reinterpret_cast<unsigned int*>(S.d_ctl + 6);
+    A.items = S.d_items;
+    A.tail = S.d_ctl + kCtlTail;
+    A.head = S.d_ctl + kCtlHead;
+    A.stop = reinterpret_cast<const unsigned int*>(S.d_ctl + kCtlStop);
+    A.live = reinterpret_cast<unsigned int*>(S.d_ctl + kCtlLive);
     A.ring_mask = kSvcRing - 1;
     A.done = S.d_done;
     A.finished = static_cast<unsigned int*>(d_fin);
@@ -3097,14 +3102,13 @@ PoaService::~PoaService() {
     {
         // the stop word ends a running kernel within its idle bound
         std::lock_guard<std::mutex> lk(S.pub_mu);
-        S.h_val[4] = 1;
-        cudaMemcpyAsync(S.d_ctl + 4, S.h_val + 4, 8, cudaMemcpyHostToDevice, S.ctl);
+        S.h_val[kCtlStop] = 1;
+        cudaMemcpyAsync(S.d_ctl + kCtlStop, S.h_val + kCtlStop, 8, cudaMemcpyHostToDevice, S.ctl);
         cudaStreamSynchronize(S.ctl);
     }
     cudaStreamSynchronize(S.stream);
     cudaFree(S.d_scratch);
-    cudaFree(S.d_items[0]);
-    cudaFree(S.d_items[1]);
+    cudaFree(S.d_items);
     cudaFree(S.d_ctl);
     cudaFree(S.d_jobs);
     cudaFree(S.d_done);
@@ -3146,18 +3150,21 @@ void PoaService::dispatcher() {
         {
             // lock order: mu, then pub_mu (publishers take pub_mu alone)
             std::lock_guard<std::mutex> plk(S.pub_mu);
-            if (S.published[0] + S.published[1] == 0) continue;
-            if (cudaMemcpyAsync(S.h_val + 2, S.d_ctl + 2, 16, cudaMemcpyDeviceToHost, S.ctl) != cudaSuccess ||
+            unsigned long long any = 0;
+            for (int q = 0; q < kSvcQueues; ++q) any += S.published[q];
+            if (any == 0) continue;
+            if (cudaMemcpyAsync(S.h_val + kCtlHead, S.d_ctl + kCtlHead, 8 * kSvcQueues, cudaMemcpyDeviceToHost,
+                                S.ctl) != cudaSuccess ||
                 cudaStreamSynchronize(S.ctl) != cudaSuccess) {
                 S.error = "rb_poa service: head read failed";
                 S.cv_slot.notify_all();
                 continue;
             }
-            pending = S.h_val[2] < S.published[0] || S.h_val[3] < S.published[1];
+            for (int q = 0; q < kSvcQueues; ++q) pending |= S.h_val[kCtlHead + q] < S.published[q];
         }
         if (!pending) continue;
         // a launch starts with no warp working and not closing
-        cudaError_t e = cudaMemsetAsync(S.d_ctl + 6, 0, 8, S.stream);
+        cudaError_t e = cudaMemsetAsync(S.d_ctl + kCtlLive, 0, 8, S.stream);
         if (e == cudaSuccess)
             poa_service_kernel<<<S.grid, 32 * kWarpsPerCta, kWarpsPerCta * kRingBytesPerWarp, S.stream>>>(S.args);
         if (e == cudaSuccess) e = cudaGetLastError();
@@ -3172,10 +3179,11 @@ void PoaService::dispatcher() {
     }
 }
 
-void PoaService::run_batch(const PoaJobDev& job, const uint32_t* order, size_t n, bool high_priority) {
+void PoaService::run_batch(const PoaJobDev& job, const uint32_t* order, size_t n, int queue) {
     PoaSvcState& S = *st_;
     if (n == 0) return;
     if (n > kSvcRing / 2) throw Error{RB_ERR_ARG, "rb_poa service: batch larger than the shared queue"};
+    if (queue < 0 || queue >= kSvcQueues) throw Error{RB_ERR_ARG, "rb_poa service: bad queue"};
     uint32_t slot = 0, gen = 0;
     {
         std::unique_lock<std::mutex> lk(S.mu);
@@ -3196,7 +3204,7 @@ void PoaService::run_batch(const PoaJobDev& job, const uint32_t* order, size_t n
         // starts from zero and its record is in place before any item is
         // visible, and the items before the tail
         std::lock_guard<std::mutex> plk(S.pub_mu);
-        const int q = high_priority ? 0 : 1;
+        const int q = queue;
         const unsigned long long t = S.published[q];
         PoaJobDev rec = job;
         rec.total = uint32_t(n);
@@ -3208,15 +3216,17 @@ void PoaService::run_batch(const PoaJobDev& job, const uint32_t* order, size_t n
         for (size_t i = 0; i < n; ++i) S.h_stage[i] = make_uint2(slot, order[i]);
         const size_t at = size_t(t & (kSvcRing - 1));
         const size_t first = std::min(n, size_t(kSvcRing) - at);
-        check_cuda(cudaMemcpyAsync(S.d_items[q] + at, S.h_stage, first * sizeof(uint2), cudaMemcpyHostToDevice,
+        uint2* ring = S.d_items + size_t(q) * kSvcRing;
+        check_cuda(cudaMemcpyAsync(ring + at, S.h_stage, first * sizeof(uint2), cudaMemcpyHostToDevice,
                                    S.ctl),
                    "H2D items");
         if (first < n)
-            check_cuda(cudaMemcpyAsync(S.d_items[q], S.h_stage + first, (n - first) * sizeof(uint2),
+            check_cuda(cudaMemcpyAsync(ring, S.h_stage + first, (n - first) * sizeof(uint2),
                                        cudaMemcpyHostToDevice, S.ctl),
                        "H2D items");
-        S.h_val[q] = t + n;
-        check_cuda(cudaMemcpyAsync(S.d_ctl + q, S.h_val + q, 8, cudaMemcpyHostToDevice, S.ctl), "H2D tail");
+        S.h_val[kCtlTail + q] = t + n;
+        check_cuda(cudaMemcpyAsync(S.d_ctl + kCtlTail + q, S.h_val + kCtlTail + q, 8, cudaMemcpyHostToDevice, S.ctl),
+                   "H2D tail");
         check_cuda(cudaStreamSynchronize(S.ctl), "service publish");
         S.published[q] = t + n;
     }
@@ -3247,7 +3257,7 @@ void PoaService::run_batch(const PoaJobDev& job, const uint32_t* order, size_t n
     if (!err.empty()) throw Error{RB_ERR_DEVICE, err};
 }
 
-void PoaEngine::run_shared(PoaService& svc, bool high_priority) {
+void PoaEngine::run_shared(PoaService& svc, uint32_t priority_windows) {
     prepare_outputs();
     const size_t n = nwin_;
     if (n == 0) return;
@@ -3265,7 +3275,10 @@ void PoaEngine::run_shared(PoaService& svc, bool high_priority) {
     job.cells = reinterpret_cast<unsigned long long*>(d_misc_.as<unsigned int>() + 8);
     job.trim = trim_;
     const auto t0 = std::chrono::steady_clock::now();
-    svc.run_batch(job, h_order_.as<uint32_t>(), n, high_priority);
+    // size class: ring 0 up to priority_windows windows, then x4 per ring
+    const uint64_t p = std::max<uint32_t>(1, priority_windows);
+    const int queue = n <= p ? 0 : n <= 4 * p ? 1 : n <= 16 * p ? 2 : 3;
+    svc.run_batch(job, h_order_.as<uint32_t>(), n, queue);
     const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     std::vector<uint8_t> flags(n);
     unsigned long long cells[2] = {0, 0};

@@ -293,7 +293,7 @@ int rb_poa_stage(rb_ctx* ctx, const rb_window* windows, size_t n, int trim) {
 int rb_poa_run(rb_ctx* ctx) {
     return guarded(ctx, [&]() {
         if (ctx->svc)
-            ctx->poa->run_shared(*ctx->svc, ctx->poa->staged() <= ctx->svc_priority_windows);
+            ctx->poa->run_shared(*ctx->svc, ctx->svc_priority_windows);
         else
             ctx->poa->run();
     });

@@ -207,8 +207,10 @@ public:
     void run(bool plain = false);
     // The staged windows through a device-wide shared queue (serving):
     // returns when every window of this batch is done; windows that outgrow
-    // the shared slots run again here with larger graph capacity.
-    void run_shared(PoaService& svc, bool high_priority);
+    // the shared slots run again here with larger graph capacity. Batches
+    // of at most priority_windows windows use the first ring, larger ones
+    // later rings (x4 per ring).
+    void run_shared(PoaService& svc, uint32_t priority_windows);
     size_t staged() const { return nwin_; }
     void fetch(rb_poa_result* out);
     const rb_stats& stats() const { return stats_; }
@@ -248,9 +250,9 @@ private:
 
 // ----- shared window-consensus service (poa_consensus.cu) -----
 // Continuous batching for the serving loop: one persistent consensus kernel
-// per device whose warps pull (job, window) items from two host-mapped
-// queues (high priority first), so windows of jobs admitted while others run
-// start as soon as any warp frees up. Jobs append their items and wait for a
+// per device whose warps pull (job, window) items from size-class rings in
+// device memory (smallest jobs first), so windows of jobs admitted while
+// others run start as soon as any warp frees up. Jobs append their items and wait for a
 // per-job completion flag; the kernel leaves after a bounded idle time and a
 // dispatcher thread relaunches it when items are pending. Thread-safe.
 struct PoaJobDev;
@@ -265,9 +267,10 @@ public:
     ~PoaService();
     PoaService(const PoaService&) = delete;
     PoaService& operator=(const PoaService&) = delete;
-    // Enqueues windows order[0..n) of the batch described by `job` and waits
-    // until all of them are done. Throws rb::Error on device failure.
-    void run_batch(const PoaJobDev& job, const uint32_t* order, size_t n, bool high_priority);
+    // Enqueues windows order[0..n) of the batch described by `job` on ring
+    // `queue` (0 is drained first) and waits until all of them are done.
+    // Throws rb::Error on device failure.
+    void run_batch(const PoaJobDev& job, const uint32_t* order, size_t n, int queue);
     uint32_t slots() const;
     uint32_t launches() const;
 
