@@ -48,6 +48,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+# Thread instructions poa_kernel executes per DP cell, from the same kind of
+# capture (smsp__inst_executed.sum x threads per instruction / DP cells:
+# 6.64 G x 30.44 / 5.84 G)
+POA_THREAD_INST_PER_CELL = 6639707327 * 30.44 / 5838774640
 # DRAM bytes (read + write) per DP cell of poa_kernel, from one ncu capture of
 # config 1 at 0.1 genome scale (1.783 GB read + 27.339 GB written over
 # 5.839 G cells); traffic grows with the cells, so a full launch's traffic is
@@ -728,6 +732,9 @@ def main():
                     "frac": achieved_tops / int_peak_tops, "gcups": gcups,
                     "edge_cells_per_step": ecells // max(1, args.steps),
                     "edge_cells_per_cell": ecells / max(1, cells),
+                    "issued_frac": cells * POA_THREAD_INST_PER_CELL / dev_s / 1e12 / int_peak_tops,
+                    "issued_note": "executed thread instructions (per DP cell from an ncu capture) / device time, "
+                                   "against the same issue peak",
                     "note": "achieved = edge-cells counted on the device (|layer| x sum_v (1 + in-degree v) over "
                             "the aligned graph) x 3 int32 ops / device time; peak = SMs x 128 int32 lanes x median "
                             "SM clock under load"},
