@@ -72,3 +72,25 @@ def test_no_silent_cpu_path_without_gpu(native_lib):
         pytest.skip("GPU present")
     with pytest.raises(native_lib.RaconB200Error):
         native_lib.Context(0)
+
+
+def test_tuning_table_clamps_and_keeps_devices_apart(native_lib):
+    # the per-device launch choices are host state: no device is needed to
+    # set and read them, values outside their ranges are clamped, and one
+    # device's choices do not touch another's
+    before = [native_lib.tuning_get(d) for d in (5, 6)]
+    try:
+        native_lib.tuning_set(5, consensus_ctas_per_sm=9, consensus_order=7, alignment_warps_per_sm=1000)
+        t = native_lib.tuning_get(5)
+        assert (t["consensus_ctas_per_sm"], t["consensus_order"], t["alignment_warps_per_sm"]) == (3, 1, 32)
+        native_lib.tuning_set(5, consensus_ctas_per_sm=0, consensus_order=0, alignment_warps_per_sm=6)
+        t = native_lib.tuning_get(5)
+        assert (t["consensus_ctas_per_sm"], t["consensus_order"], t["alignment_warps_per_sm"]) == (1, 0, 4)
+        assert native_lib.tuning_get(6) == before[1]
+    finally:
+        native_lib.tuning_set(5, **before[0])
+
+
+def test_tuning_defaults(native_lib):
+    t = native_lib.tuning_get(7)
+    assert (t["consensus_ctas_per_sm"], t["consensus_order"], t["alignment_warps_per_sm"], t["tuned"]) == (3, 0, 16, 0)
