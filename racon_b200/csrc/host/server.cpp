@@ -7,18 +7,19 @@
 //     buffers). Buffers grow to the largest job a worker has run and stay
 //     allocated; growth is stream-ordered, so it does not synchronise the
 //     device under the other workers.
-//   - Jobs on different workers overlap on the device: one job's host stages
-//     (parsing, layer assembly, stitching) run while another's kernels run,
-//     and the kernels of concurrent jobs share the SMs as CTAs retire. (The
-//     contexts' kernels stay persistent on all SMs: bounded work per launch
-//     with small jobs on the high-priority stream, rb_set_yield /
-//     rb_set_priority, and large jobs on 70 % of the SMs, rb_set_sm_share,
-//     both measured worse for the p99 latency ratio.)
+//   - Continuous batching of the window consensus: one PoaService per server
+//     (a persistent consensus kernel on part of every SM, fed by size-class
+//     rings in device memory). A worker runs its job's parsing, alignment and
+//     layer assembly on its own context, then its rb_poa_run appends the
+//     job's windows to the shared queue and waits; windows of jobs admitted
+//     while others run start on the next free warp.
+//   - Optional (alignment_yield): small jobs on the high-priority stream and
+//     large jobs' alignment in bounded launches, so a small job's alignment
+//     kernels find SMs between a large job's launches.
 //   - Admission is first in first out by estimated device footprint: the
 //     head of the queue starts when a worker is idle and its estimate fits
 //     beside the jobs in flight within hbm_budget (a job alone always
-//     starts). Each worker's window-consensus scratch is capped at
-//     hbm_budget / workers, which bounds the real allocation too.
+//     starts).
 #include <cuda_runtime.h>
 #include <sys/stat.h>
 

@@ -2466,7 +2466,7 @@ struct PoaSvcArgs {
     unsigned long long idle_ns;      // a warp leaves after this long without work
 };
 
-// Claims the next item, high-priority ring first: returns (job << 32) |
+// Claims the next item, ring 0 (smallest jobs) first: returns (job << 32) |
 // window, or ~0 when the kernel closes or stop is set. The kernel closes as a
 // whole: a warp that has found no work for idle_ns while no warp of the
 // kernel is working sets the closing word, and every warp leaves at its next

@@ -63,8 +63,8 @@ def test_server_bad_job_fails_alone(native_lib):
 def test_server_jobs_join_running_kernel(native_lib, tmp_path):
     """Continuous batching: a long job keeps the shared consensus kernel busy
     while small jobs arrive one by one; each small job's windows join the
-    running kernel (high-priority queue) and every output equals the job run
-    alone, including the long one."""
+    running kernel (through the first, smallest-jobs ring) and every output
+    equals the job run alone, including the long one."""
     from racon_b200 import synthetic
     r, o, t, _ = synthetic.contig(str(tmp_path / "big"), 1, scale=0.08)
     big_alone = native_lib.polish_files(r, o, t, match=5, mismatch=-4, gap=-8)
