@@ -85,6 +85,8 @@ def _args():
                    help="serving: each job launches its own consensus kernel")
     p.add_argument("--alignment-yield", type=int, default=0,
                    help="serving: alignment pairs per warp and launch for large jobs (0: persistent)")
+    p.add_argument("--alignment-share", type=int, default=0,
+                   help="serving: percent of the SMs large jobs' alignment grids fill (0: all)")
     p.add_argument("--pairs", type=int, default=10000, help="config-2 pairs per step")
     return p.parse_args()
 
@@ -266,6 +268,7 @@ def run_serving(args, device, rates):
     out["hbm_budget"] = budget
     out["shared_consensus"] = not args.no_shared_consensus
     out["alignment_yield"] = args.alignment_yield
+    out["alignment_share"] = args.alignment_share
     t_start = time.perf_counter()
 
     def log(msg):
@@ -274,7 +277,8 @@ def run_serving(args, device, rates):
 
     with racon_b200.Server(device, workers=args.workers, hbm_budget=budget, match=3, mismatch=-5, gap=-4,
                            window_length=w, shared_consensus=not args.no_shared_consensus,
-                           alignment_yield=args.alignment_yield) as srv:
+                           alignment_yield=args.alignment_yield,
+                           alignment_share=args.alignment_share) as srv:
         def run(arrivals):
             t0 = time.perf_counter()
             tickets = []
@@ -297,11 +301,12 @@ def run_serving(args, device, rates):
         for t in [srv.submit(*jobs[big][:3]) for _ in range(args.workers)]:
             srv.wait(t)
         log("workers warmed with the largest job")
-        iso, alone = [], []
+        iso, alone, iso_stage = [], [], []
         for j in jobs:
             fasta, tm = srv.wait(srv.submit(j[0], j[1], j[2]))
             alone.append(fasta)
             iso.append(tm["finished"] - tm["submitted"])
+            iso_stage.append(tm["stage_seconds"])
         log("isolated runs done, sum %.2f s" % sum(iso))
         fastas, _, span = run(None)
         assert fastas == alone, "a job's output differs between alone and in the mix"
@@ -326,12 +331,17 @@ def run_serving(args, device, rates):
             wait = [tm["admitted"] - tm["submitted"] for tm in times]
             stages = [[tm["stage_seconds"][k] for tm in times] for k in range(4)]
             log("load %.2f done, makespan %.2f s, p99 latency %.2f s" % (frac, span, _pct(lat, 99)))
+            worst = max(range(len(jobs)), key=lambda k: ratio[k])
             sweep.append({"load": frac, "jobs_per_s": len(jobs) / span, "windows_per_s": sum(windows) / span,
                           "latency_s": {"p50": _pct(lat, 50), "p99": _pct(lat, 99)},
                           "latency_vs_isolated": {"p50": _pct(ratio, 50), "p99": _pct(ratio, 99)},
                           "admission_wait_s": {"mean": sum(wait) / len(wait), "max": max(wait)},
                           "stage_mean_s": [sum(x) / len(x) for x in stages],
-                          "stage_max_s": [max(x) for x in stages]})
+                          "stage_max_s": [max(x) for x in stages],
+                          "worst_job": {"windows": windows[worst], "isolated_s": iso[worst], "latency_s": lat[worst],
+                                        "admission_wait_s": wait[worst],
+                                        "stage_s": [stages[k][worst] for k in range(4)],
+                                        "isolated_stage_s": list(iso_stage[worst])}})
         out["rates"] = sweep
     return out
 

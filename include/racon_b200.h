@@ -392,7 +392,9 @@ void rb_free(void* p);
  * alignment_yield > 0 puts jobs of at most priority_windows windows on the
  * high-priority stream and bounds the alignment work of larger jobs to that
  * many pairs per warp and launch, so that a small job's alignment kernels
- * find free SMs between a large job's launches (results unchanged). */
+ * find free SMs between a large job's launches. alignment_share (1..99, 0:
+ * 100) sizes larger jobs' persistent alignment grids for that percent of
+ * the SMs, leaving the rest to small jobs' alignment (results unchanged). */
 typedef struct rb_server_params {
     int device;
     uint32_t workers;
@@ -405,6 +407,7 @@ typedef struct rb_server_params {
     uint32_t consensus_ctas_per_sm;
     uint32_t priority_windows;
     uint32_t alignment_yield;
+    uint32_t alignment_share;
 } rb_server_params;
 
 /* One job: racon's inputs and per-job flags (-f, -q, -e, --no-trimming, -u). */

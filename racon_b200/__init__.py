@@ -93,7 +93,7 @@ class _ServerParams(ctypes.Structure):
                 ("match", ctypes.c_int8), ("mismatch", ctypes.c_int8), ("gap", ctypes.c_int8),
                 ("window_length", ctypes.c_uint32), ("shared_consensus", ctypes.c_int),
                 ("consensus_ctas_per_sm", ctypes.c_uint32), ("priority_windows", ctypes.c_uint32),
-                ("alignment_yield", ctypes.c_uint32)]
+                ("alignment_yield", ctypes.c_uint32), ("alignment_share", ctypes.c_uint32)]
 
 
 class _ServerJob(ctypes.Structure):
@@ -630,10 +630,11 @@ class Server:
     first. submit() returns a ticket; wait(ticket) returns (fasta, times)."""
 
     def __init__(self, device=0, workers=4, hbm_budget=0, match=3, mismatch=-5, gap=-4, window_length=500,
-                 shared_consensus=True, consensus_ctas_per_sm=0, priority_windows=0, alignment_yield=0):
+                 shared_consensus=True, consensus_ctas_per_sm=0, priority_windows=0, alignment_yield=0,
+                 alignment_share=0):
         self.lib = load()
         p = _ServerParams(device, workers, hbm_budget, match, mismatch, gap, window_length, int(shared_consensus),
-                          consensus_ctas_per_sm, priority_windows, alignment_yield)
+                          consensus_ctas_per_sm, priority_windows, alignment_yield, alignment_share)
         self.ptr = self.lib.rb_server_create(ctypes.byref(p))
         if not self.ptr:
             msg = self.lib.rb_server_error().decode() or self.lib.rb_create_error().decode()
