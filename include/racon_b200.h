@@ -394,7 +394,8 @@ void rb_free(void* p);
  * many pairs per warp and launch, so that a small job's alignment kernels
  * find free SMs between a large job's launches. alignment_share (1..99, 0:
  * 100) sizes larger jobs' persistent alignment grids for that percent of
- * the SMs, leaving the rest to small jobs' alignment (results unchanged). */
+ * the SMs (and also puts small jobs on the high-priority stream), leaving
+ * the rest to small jobs' alignment. Results are unchanged either way. */
 typedef struct rb_server_params {
     int device;
     uint32_t workers;

@@ -130,17 +130,12 @@ struct rb_server {
             double stage[4] = {0, 0, 0, 0};
             const rb_server_job& j = r->spec;
             const bool small = r->windows <= params.priority_windows;
-            if (params.alignment_yield) {
-                // small jobs on the high-priority stream with persistent
-                // alignment kernels; large jobs give the SMs back between
-                // bounded launches
-                rb_set_priority(ctxs[w], small ? 1 : 0);
-                rb_set_yield(ctxs[w], 0, small ? 0u : params.alignment_yield);
-            }
-            if (params.alignment_share) {
-                // large jobs' persistent alignment grids on part of the SMs
-                rb_set_sm_share(ctxs[w], small ? 100u : params.alignment_share);
-            }
+            // small jobs on the high-priority stream; large jobs give SMs
+            // back between bounded alignment launches, or keep their
+            // persistent alignment grids to part of the SMs
+            if (params.alignment_yield || params.alignment_share) rb_set_priority(ctxs[w], small ? 1 : 0);
+            if (params.alignment_yield) rb_set_yield(ctxs[w], 0, small ? 0u : params.alignment_yield);
+            if (params.alignment_share) rb_set_sm_share(ctxs[w], small ? 100u : params.alignment_share);
             const int rc = racon::polish_job_on_context(
                 ctxs[w], params.device, r->sp, r->op, r->tp, j.fragment != 0, params.window_length,
                 j.quality_threshold, j.error_threshold, j.trim != 0, params.match, params.mismatch, params.gap,
