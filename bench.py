@@ -83,6 +83,10 @@ def _args():
     p.add_argument("--workers", type=int, default=8, help="serving-loop workers")
     p.add_argument("--no-shared-consensus", action="store_true",
                    help="serving: each job launches its own consensus kernel")
+    p.add_argument("--no-shared-alignment", action="store_true",
+                   help="serving: each job launches its own alignment kernels")
+    p.add_argument("--alignment-ctas", type=int, default=0,
+                   help="serving: CTAs per SM of the shared alignment kernel (0: 1)")
     p.add_argument("--alignment-yield", type=int, default=0,
                    help="serving: alignment pairs per warp and launch for large jobs (0: persistent)")
     p.add_argument("--alignment-share", type=int, default=0,
@@ -267,6 +271,8 @@ def run_serving(args, device, rates):
     budget = int(free_b * 0.7)
     out["hbm_budget"] = budget
     out["shared_consensus"] = not args.no_shared_consensus
+    out["shared_alignment"] = not args.no_shared_alignment
+    out["alignment_ctas_per_sm"] = args.alignment_ctas or 1
     out["alignment_yield"] = args.alignment_yield
     out["alignment_share"] = args.alignment_share
     t_start = time.perf_counter()
@@ -278,7 +284,9 @@ def run_serving(args, device, rates):
     with racon_b200.Server(device, workers=args.workers, hbm_budget=budget, match=3, mismatch=-5, gap=-4,
                            window_length=w, shared_consensus=not args.no_shared_consensus,
                            alignment_yield=args.alignment_yield,
-                           alignment_share=args.alignment_share) as srv:
+                           alignment_share=args.alignment_share,
+                           shared_alignment=not args.no_shared_alignment,
+                           alignment_ctas_per_sm=args.alignment_ctas) as srv:
         def run(arrivals):
             t0 = time.perf_counter()
             tickets = []

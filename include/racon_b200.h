@@ -395,7 +395,18 @@ void rb_free(void* p);
  * find free SMs between a large job's launches. alignment_share (1..99, 0:
  * 100) sizes larger jobs' persistent alignment grids for that percent of
  * the SMs (and also puts small jobs on the high-priority stream), leaving
- * the rest to small jobs' alignment. Results are unchanged either way. */
+ * the rest to small jobs' alignment. Both apply only to jobs aligned on
+ * their own kernels.
+ *
+ * Overlap alignment is continuously batched the same way when
+ * shared_alignment is set: one persistent alignment kernel per server takes
+ * the distance passes and path-recursion levels of every job in flight from
+ * its own four rings, drained smallest first (up to priority_pairs pairs, 0:
+ * the kernel's resident warps; then 4x, 16x and larger). A job waits for
+ * each level before publishing the next. alignment_ctas_per_sm (0: 1) sizes
+ * the kernel (4 warps per CTA). Its scratch is sized for spans up to
+ * alignment_max_span bases (0: 131072); a job with a longer query or target
+ * span aligns on its own kernels. Results are unchanged either way. */
 typedef struct rb_server_params {
     int device;
     uint32_t workers;
@@ -409,6 +420,10 @@ typedef struct rb_server_params {
     uint32_t priority_windows;
     uint32_t alignment_yield;
     uint32_t alignment_share;
+    int shared_alignment;
+    uint32_t alignment_ctas_per_sm;
+    uint32_t alignment_max_span;
+    uint32_t priority_pairs;
 } rb_server_params;
 
 /* One job: racon's inputs and per-job flags (-f, -q, -e, --no-trimming, -u). */

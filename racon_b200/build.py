@@ -24,8 +24,8 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-Wextra", "-pthread",
              "-I/usr/local/cuda/include"]
 
 CU_SOURCES = ["nw_align.cu", "poa_consensus.cu", "layers.cu"]
-CXX_SOURCES = ["rb_capi.cpp", "host/polisher.cpp", "host/server.cpp"]
-HEADERS = ["rb_internal.hpp", "host/racon.hpp", os.path.join("..", "..", "include", "racon_b200.h")]
+CXX_SOURCES = ["rb_capi.cpp", "ring_service.cpp", "host/polisher.cpp", "host/server.cpp"]
+HEADERS = ["rb_internal.hpp", "ring_queue.cuh", "host/racon.hpp", os.path.join("..", "..", "include", "racon_b200.h")]
 
 
 def _newer(target, deps):

@@ -13,9 +13,17 @@
 //     layer assembly on its own context, then its rb_poa_run appends the
 //     job's windows to the shared queue and waits; windows of jobs admitted
 //     while others run start on the next free warp.
-//   - Optional (alignment_yield): small jobs on the high-priority stream and
-//     large jobs' alignment in bounded launches, so a small job's alignment
-//     kernels find SMs between a large job's launches.
+//   - Continuous batching of the overlap alignment (shared_alignment): one
+//     NwService per server, a persistent alignment kernel on one CTA per SM
+//     by default, fed by its own size-class rings. A job's distance pass and
+//     each level of its path recursion are batches of that queue, so a small
+//     job's pairs start on the next free warp instead of waiting for a large
+//     job's persistent alignment grid to drain. Jobs whose spans exceed the
+//     kernel's scratch align on their own context.
+//   - Optional, for jobs aligned on their own context (alignment_yield):
+//     small jobs on the high-priority stream and large jobs' alignment in
+//     bounded launches, so a small job's alignment kernels find SMs between
+//     a large job's launches.
 //   - Admission is first in first out by estimated device footprint: the
 //     head of the queue starts when a worker is idle and its estimate fits
 //     beside the jobs in flight within hbm_budget (a job alone always
@@ -74,7 +82,8 @@ struct rb_server {
     rb_server_params params{};
     int sm_count = 148;
     uint64_t poa_cap = 0;
-    std::unique_ptr<rb::PoaService> svc;  // shared consensus kernel (continuous batching)
+    std::unique_ptr<rb::PoaService> svc;    // shared consensus kernel (continuous batching)
+    std::unique_ptr<rb::NwService> nw_svc;  // shared alignment kernel
     std::vector<rb_ctx*> ctxs;
     std::vector<std::thread> threads;
     std::mutex mu;
@@ -206,6 +215,20 @@ rb_server* rb_server_create(const rb_server_params* params) {
             rb::ctx_set_poa_service(c, s->svc.get(), prio);
         }
     }
+    if (s->params.shared_alignment) {
+        const uint32_t cps = s->params.alignment_ctas_per_sm ? s->params.alignment_ctas_per_sm : 1;
+        const uint32_t span = s->params.alignment_max_span ? s->params.alignment_max_span : 131072;
+        try {
+            s->nw_svc.reset(new rb::NwService(params->device, span, size_t(4) << 30, cps));
+        } catch (const rb::Error& e) {
+            s->svc.reset();
+            for (rb_ctx* x : s->ctxs) rb_destroy(x);
+            t_server_error = e.msg;
+            return nullptr;
+        }
+        if (s->params.priority_pairs == 0) s->params.priority_pairs = s->nw_svc->slots();
+        for (rb_ctx* c : s->ctxs) rb::ctx_set_nw_service(c, s->nw_svc.get(), s->params.priority_pairs);
+    }
     for (uint32_t i = 0; i < s->params.workers; ++i) s->threads.emplace_back([srv = s.get(), i] { srv->worker(i); });
     return s.release();
 }
@@ -319,6 +342,7 @@ void rb_server_destroy(rb_server* s) {
     for (auto& t : s->threads) t.join();
     for (rb_ctx* c : s->ctxs) rb_destroy(c);
     s->svc.reset();
+    s->nw_svc.reset();
     delete s;
 }
 

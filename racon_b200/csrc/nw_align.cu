@@ -42,16 +42,19 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <thread>
 #include <vector>
 
 #include "rb_internal.hpp"
+#include "ring_queue.cuh"
 
 namespace rb {
 namespace {
@@ -582,6 +585,59 @@ __device__ __forceinline__ bool is_leaf(uint32_t m, uint32_t n) {
 
 extern __shared__ u64 g_peq_smem[];
 
+// Edit distance of pair pi by one warp (k doubling from max(64, |m - n|)),
+// and, from lane 0, the pair's root task of the path recursion when both
+// sides are non-empty (edlib returns no alignment for an empty side).
+__device__ void distance_pair(const NwDevArgs& a, uint32_t pi, const WarpScratch& ws, u64* peq, int lane) {
+    const NwPairDev P = a.pairs[pi];
+    const int m = int(P.m), n = int(P.n);
+    if (m == 0 || n == 0) {
+        if (lane == 0) a.dist[pi] = max(m, n);
+        return;
+    }
+    SweepIO io;
+    io.q = a.codes + P.q_off;
+    io.t = a.codes + P.t_off;
+    io.rev = false;
+    io.ncols = n;
+    io.nsym = int(P.nsym);
+    io.peq = int(P.nsym) > kMaxSym ? peq_wide(ws) : peq;
+    io.leaf = nullptr;
+    io.bw = 0;
+    int k = max(64, abs(m - n));
+    int d = INT_MAX;
+    while (true) {
+        const Band B = make_band(m, n, k);
+        SweepFail f;
+        d = warp_sweep<kDistance>(io, B, ws, lane, a.counters, &f);
+        if (d <= k) break;
+        k = next_k(k, f, m, n);
+    }
+    if (lane == 0) {
+        a.dist[pi] = d;
+        const unsigned idx = atomicAdd(&a.counters[1], 1u);
+        if (idx < a.tasks_out_cap) {
+            a.tasks_out[idx] = NwTask{pi, 0, P.m, 0, P.n, d};
+        } else {
+            set_status(a.counters, kNwTaskOverflow);
+        }
+    }
+}
+
+// Task i of the current recursion level: traceback of a leaf, or a
+// Hirschberg split that appends the two halves to the next level.
+__device__ void level_task(const NwDevArgs& a, uint32_t i, const WarpScratch& ws, u64* peq, int lane) {
+    const NwTask T = a.tasks_in[i];
+    const NwPairDev P = a.pairs[T.pair];
+    if (is_leaf(T.m, T.n)) {
+        leaf_traceback(a, P, T, ws, peq, lane);
+    } else {
+        hirschberg_split(a, P, T, ws, peq, lane);
+    }
+}
+
+// Persistent distance pass of one engine: pairs in size order from an
+// atomic cursor.
 __global__ void __launch_bounds__(32 * kWarpsPerBlock)
 nw_distance_kernel(NwDevArgs a) {
     const int lane = threadIdx.x & 31;
@@ -594,49 +650,11 @@ nw_distance_kernel(NwDevArgs a) {
         if (lane == 0) i = atomicAdd(&a.counters[0], 1u);
         i = __shfl_sync(kFull, i, 0);
         if (i >= a.npairs) break;
-        const uint32_t pi = a.order[i];
-        const NwPairDev P = a.pairs[pi];
-        const int m = int(P.m), n = int(P.n);
-        if (m == 0 || n == 0) {
-            if (lane == 0) a.dist[pi] = max(m, n);
-            continue;
-        }
-        SweepIO io;
-        io.q = a.codes + P.q_off;
-        io.t = a.codes + P.t_off;
-        io.rev = false;
-        io.ncols = n;
-        io.nsym = int(P.nsym);
-        io.peq = peq;
-        if (int(P.nsym) > kMaxSym) io.peq = peq_wide(warp_scratch(a, slot));
-        io.leaf = nullptr;
-        io.bw = 0;
-        int k = max(64, abs(m - n));
-        int d = INT_MAX;
-        while (true) {
-            const Band B = make_band(m, n, k);
-            SweepFail f;
-            d = warp_sweep<kDistance>(io, B, ws, lane, a.counters, &f);
-            if (d <= k) break;
-            k = next_k(k, f, m, n);
-        }
-        if (lane == 0) a.dist[pi] = d;
+        distance_pair(a, a.order[i], ws, peq, lane);
     }
 }
 
-__global__ void nw_root_tasks_kernel(NwDevArgs a) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.npairs) return;
-    const NwPairDev P = a.pairs[i];
-    if (P.m == 0 || P.n == 0) return;  // edlib returns no alignment for an empty side
-    const unsigned idx = atomicAdd(&a.counters[1], 1u);
-    if (idx < a.tasks_out_cap) {
-        a.tasks_out[idx] = NwTask{i, 0, P.m, 0, P.n, a.dist[i]};
-    } else {
-        set_status(a.counters, kNwTaskOverflow);
-    }
-}
-
+// One recursion level of one engine: tasks from an atomic cursor.
 __global__ void __launch_bounds__(32 * kWarpsPerBlock)
 nw_level_kernel(NwDevArgs a) {
     const int lane = threadIdx.x & 31;
@@ -649,14 +667,90 @@ nw_level_kernel(NwDevArgs a) {
         if (lane == 0) i = atomicAdd(&a.counters[0], 1u);
         i = __shfl_sync(kFull, i, 0);
         if (i >= a.ntasks_in) break;
-        const NwTask T = a.tasks_in[i];
-        const NwPairDev P = a.pairs[T.pair];
-        if (is_leaf(T.m, T.n)) {
-            leaf_traceback(a, P, T, ws, peq, lane);
-        } else {
-            hirschberg_split(a, P, T, ws, peq, lane);
-        }
+        level_task(a, i, ws, peq, lane);
         __syncwarp();
+    }
+}
+
+}  // namespace
+
+// One batch of the shared alignment queue (device record, written before
+// its items are published): a distance pass over pairs, or one recursion
+// level over tasks, of one engine's staged pairs.
+struct NwJobDev {
+    SvcJobHead head;
+    uint32_t mode;           // 0: items are pair indices (distance), 1: task indices (level)
+    uint32_t ntasks_in;
+    uint32_t tasks_out_cap;
+    uint32_t pad;
+    const uint8_t* codes;
+    const NwPairDev* pairs;
+    int32_t* dist;
+    int32_t* mq;
+    unsigned int* counters;  // [1] tasks appended to tasks_out, [2] status
+    const void* tasks_in;    // NwTask records of the level
+    void* tasks_out;         // NwTask records of the next level
+};
+
+namespace {
+
+constexpr uint32_t kJobDistance = 0, kJobLevel = 1;
+
+// The alignment service's kernel arguments: the warps' scratch (sized for
+// the service's longest span), the batch records, and the queue.
+struct NwSvcArgs {
+    NwDevArgs base;
+    const NwJobDev* jobs;
+    SvcQueueDev q;
+};
+
+// Persistent alignment over the shared queue: each warp owns one scratch
+// slot and takes distance passes and recursion tasks of any job until the
+// queue stays empty.
+__global__ void __launch_bounds__(32 * kWarpsPerBlock)
+nw_service_kernel(NwSvcArgs s) {
+    __shared__ NwDevArgs a_all[kWarpsPerBlock];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const uint32_t slot = blockIdx.x * kWarpsPerBlock + wib;
+    u64* peq = g_peq_smem + wib * kMaxSym * 32;
+    const WarpScratch ws = warp_scratch(s.base, slot);
+    for (;;) {
+        unsigned long long it = 0;
+        if (lane == 0) it = svc_claim(s.q);
+        it = __shfl_sync(kFull, it, 0);
+        if (it == ~0ull) break;
+        const uint32_t job = uint32_t(it >> 32), idx = uint32_t(it);
+        uint32_t mode = 0, total = 0, gen = 0;
+        if (lane == 0) {
+            // the record is rewritten for every batch that reuses the slot:
+            // read it past L1
+            const volatile NwJobDev& J = s.jobs[job];
+            NwDevArgs a = s.base;
+            a.codes = const_cast<const uint8_t*>(J.codes);
+            a.pairs = const_cast<const NwPairDev*>(J.pairs);
+            a.dist = const_cast<int32_t*>(J.dist);
+            a.mq = const_cast<int32_t*>(J.mq);
+            a.counters = const_cast<unsigned int*>(J.counters);
+            a.tasks_in = static_cast<const NwTask*>(const_cast<const void*>(J.tasks_in));
+            a.ntasks_in = J.ntasks_in;
+            a.tasks_out = static_cast<NwTask*>(const_cast<void*>(J.tasks_out));
+            a.tasks_out_cap = J.tasks_out_cap;
+            mode = J.mode;
+            total = J.head.total;
+            gen = J.head.generation;
+            a_all[wib] = a;
+        }
+        mode = __shfl_sync(kFull, mode, 0);
+        __syncwarp();
+        if (mode == kJobDistance) {
+            distance_pair(a_all[wib], idx, ws, peq, lane);
+        } else {
+            level_task(a_all[wib], idx, ws, peq, lane);
+        }
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) svc_item_done(s.q, job, total, gen);
     }
 }
 
@@ -1108,7 +1202,6 @@ NwEngine::NwEngine(const DeviceInfo& dev, cudaStream_t stream) : dev_(dev), stre
                                     kWarpsPerBlock * kMaxSym * 32 * 8),
                "cudaFuncSetAttribute");
     const void* kernels[] = {reinterpret_cast<const void*>(nw_distance_kernel),
-                             reinterpret_cast<const void*>(nw_root_tasks_kernel),
                              reinterpret_cast<const void*>(nw_level_kernel),
                              reinterpret_cast<const void*>(nw_breakpoints_kernel),
                              reinterpret_cast<const void*>(nw_cigar_kernel),
@@ -1352,6 +1445,36 @@ void NwEngine::reserve_scratch(uint32_t max_m, uint32_t max_n) {
 }
 
 void NwEngine::run() {
+    if (svc_ && npairs_ > 0 && svc_->fits(max_m_, max_n_)) {
+        run_shared();
+    } else {
+        run_own();
+    }
+}
+
+namespace {
+// Arguments of the staged batch common to the engine's own kernels and the
+// shared service (scratch and queue fields are set by the caller).
+NwDevArgs batch_args(const DevBuf& codes, const DevBuf& pairs, const DevBuf& order, size_t n, const DevBuf& dist,
+                     const DevBuf& mq, const DevBuf& bp, const DevBuf& bpcnt, uint32_t window_length,
+                     const DevBuf& misc) {
+    NwDevArgs a;
+    memset(&a, 0, sizeof(a));
+    a.codes = codes.as<uint8_t>();
+    a.pairs = pairs.as<NwPairDev>();
+    a.order = order.as<uint32_t>();
+    a.npairs = uint32_t(n);
+    a.dist = dist.as<int32_t>();
+    a.mq = mq.as<int32_t>();
+    a.bp = bp.as<uint32_t>();
+    a.bp_count = bpcnt.as<uint32_t>();
+    a.window_length = window_length;
+    a.counters = misc.as<unsigned int>();
+    return a;
+}
+}  // namespace
+
+void NwEngine::run_own() {
     const size_t n = npairs_;
     stats_.launches = 0;
     stats_.items = n;
@@ -1364,23 +1487,16 @@ void NwEngine::run() {
     size_t task_cap = std::max<size_t>(n, 1) * 2 + 64;
     d_tasks_[0].reserve(task_cap * sizeof(NwTask));
     d_tasks_[1].reserve(task_cap * sizeof(NwTask));
-    NwDevArgs a;
-    memset(&a, 0, sizeof(a));
-    a.codes = d_codes_.as<uint8_t>();
-    a.pairs = d_pairs_.as<NwPairDev>();
-    a.order = d_order_.as<uint32_t>();
-    a.npairs = uint32_t(n);
-    a.dist = d_dist_.as<int32_t>();
-    a.mq = d_mq_.as<int32_t>();
-    a.bp = d_bp_.as<uint32_t>();
-    a.bp_count = d_bpcnt_.as<uint32_t>();
-    a.window_length = window_length_;
+    NwDevArgs a = batch_args(d_codes_, d_pairs_, d_order_, n, d_dist_, d_mq_, d_bp_, d_bpcnt_, window_length_,
+                             d_misc_);
     a.scratch = d_scratch_.as<uint8_t>();
     a.scratch_stride = scratch_stride_;
     a.scratch_warps = uint32_t(scratch_warps_);
     a.max_n = max_n_ + 64;
     a.max_nb = (max_m_ + 63) / 64 + 1;
-    a.counters = d_misc_.as<unsigned int>();
+    // the distance pass appends each pair's root task (level 0)
+    a.tasks_out = d_tasks_[0].as<NwTask>();
+    a.tasks_out_cap = uint32_t(task_cap);
     const int grid = int(scratch_warps_ / kWarpsPerBlock);
     const size_t smem = kWarpsPerBlock * kMaxSym * 32 * 8;
     check_cuda(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
@@ -1396,11 +1512,6 @@ void NwEngine::run() {
         nw_distance_kernel<<<grid, 32 * kWarpsPerBlock, smem, stream_>>>(a);
         ++stats_.launches;
     }
-    // level 0 tasks
-    a.tasks_out = d_tasks_[0].as<NwTask>();
-    a.tasks_out_cap = uint32_t(task_cap);
-    nw_root_tasks_kernel<<<int((n + 255) / 256), 256, 0, stream_>>>(a);
-    ++stats_.launches;
     unsigned int h_cnt[4];
     check_cuda(cudaMemcpyAsync(h_cnt, a.counters, 16, cudaMemcpyDeviceToHost, stream_), "D2H count");
     check_cuda(cudaStreamSynchronize(stream_), "sync level");
@@ -1426,6 +1537,86 @@ void NwEngine::run() {
         ntasks = h_cnt[1];
         cur ^= 1;
     }
+    finish_outputs(&a);
+    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    check_cuda(cudaStreamSynchronize(stream_), "sync run");
+    check_cuda(cudaGetLastError(), "nw kernels");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.kernel_ms = ms;
+}
+
+// The distance pass and every recursion level as batches of the shared
+// service (each waits for the previous one: a level's tasks come from the
+// one before), then the breaking points (and CIGARs) on this engine's stream.
+void NwEngine::run_shared() {
+    const size_t n = npairs_;
+    stats_.launches = 0;
+    stats_.items = n;
+    stats_.cells = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    size_t task_cap = std::max<size_t>(n, 1) * 2 + 64;
+    d_tasks_[0].reserve(task_cap * sizeof(NwTask));
+    d_tasks_[1].reserve(task_cap * sizeof(NwTask));
+    NwDevArgs a = batch_args(d_codes_, d_pairs_, d_order_, n, d_dist_, d_mq_, d_bp_, d_bpcnt_, window_length_,
+                             d_misc_);
+    check_cuda(cudaMemsetAsync(a.counters, 0, 64, stream_), "memset counters");
+    // the staged pairs and the counters are in place before any item is published
+    check_cuda(cudaStreamSynchronize(stream_), "nw stage sync");
+    NwJobDev job;
+    memset(&job, 0, sizeof(job));
+    job.mode = kJobDistance;
+    job.codes = a.codes;
+    job.pairs = a.pairs;
+    job.dist = a.dist;
+    job.mq = a.mq;
+    job.counters = a.counters;
+    job.tasks_out = d_tasks_[0].ptr;
+    job.tasks_out_cap = uint32_t(task_cap);
+    // size class: ring 0 up to svc_priority_ pairs, then x4 per ring
+    const uint64_t p = std::max<uint32_t>(1, svc_priority_);
+    const int queue = n <= p ? 0 : n <= 4 * p ? 1 : n <= 16 * p ? 2 : 3;
+    svc_->run_batch(job, h_order_.as<uint32_t>(), n, queue);
+    ++stats_.launches;
+    unsigned int h_cnt[4];
+    check_cuda(cudaMemcpyAsync(h_cnt, a.counters, 16, cudaMemcpyDeviceToHost, stream_), "D2H count");
+    check_cuda(cudaStreamSynchronize(stream_), "sync level");
+    if (h_cnt[2] != 0) throw Error{RB_ERR_DEVICE, "nw: distance pass status " + std::to_string(h_cnt[2])};
+    uint32_t ntasks = h_cnt[1];
+    std::vector<uint32_t> idx;
+    int cur = 0;
+    while (ntasks > 0) {
+        const size_t need = size_t(ntasks) * 2 + 64;
+        d_tasks_[cur ^ 1].reserve(need * sizeof(NwTask));
+        task_cap = d_tasks_[cur ^ 1].bytes / sizeof(NwTask);
+        check_cuda(cudaMemsetAsync(a.counters, 0, 8, stream_), "memset counters");
+        check_cuda(cudaStreamSynchronize(stream_), "nw level sync");
+        job.mode = kJobLevel;
+        job.tasks_in = d_tasks_[cur].ptr;
+        job.ntasks_in = ntasks;
+        job.tasks_out = d_tasks_[cur ^ 1].ptr;
+        job.tasks_out_cap = uint32_t(task_cap);
+        idx.resize(ntasks);
+        std::iota(idx.begin(), idx.end(), 0u);
+        svc_->run_batch(job, idx.data(), ntasks, queue);
+        ++stats_.launches;
+        check_cuda(cudaMemcpyAsync(h_cnt, a.counters, 16, cudaMemcpyDeviceToHost, stream_), "D2H count");
+        check_cuda(cudaStreamSynchronize(stream_), "sync level");
+        if (h_cnt[2] != 0) throw Error{RB_ERR_DEVICE, "nw: level pass status " + std::to_string(h_cnt[2])};
+        ntasks = h_cnt[1];
+        cur ^= 1;
+    }
+    finish_outputs(&a);
+    check_cuda(cudaStreamSynchronize(stream_), "sync run");
+    check_cuda(cudaGetLastError(), "nw kernels");
+    stats_.kernel_ms = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+}
+
+// Breaking points, and with want_cigar the CIGAR strings, of the aligned
+// pairs: warp-per-pair kernels on this engine's stream.
+void NwEngine::finish_outputs(const void* args) {
+    const NwDevArgs& a = *static_cast<const NwDevArgs*>(args);
+    const size_t n = npairs_;
     const int warp_grid = int(std::max<size_t>(1, std::min<size_t>((n + 7) / 8, size_t(dev_.sm_count) * 16)));
     nw_breakpoints_kernel<<<warp_grid, 256, 0, stream_>>>(a);
     ++stats_.launches;
@@ -1443,16 +1634,9 @@ void NwEngine::run() {
         d_cig_.reserve(std::max<uint64_t>(total, 1));
         nw_cigar_kernel<<<warp_grid, 256, 0, stream_>>>(a, d_ciglen_.as<uint64_t>(),
                                                                    d_cigoff_.as<uint64_t>(), d_cig_.as<char>(), 1);
-        stats_.launches += 4;
+        stats_.launches += 3;
     }
-    check_cuda(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
-    check_cuda(cudaStreamSynchronize(stream_), "sync run");
-    check_cuda(cudaGetLastError(), "nw kernels");
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ev0_, ev1_);
-    stats_.kernel_ms = ms;
 }
-
 
 void NwEngine::cigar_breakpoints(const rb_cigar_overlap* ovl, size_t n, uint32_t w, rb_aln_result* out) {
     if (n > 0 && !ovl) throw Error{RB_ERR_ARG, "rb_cigar_breakpoints: overlaps is NULL"};
@@ -1590,6 +1774,74 @@ void NwEngine::fetch(rb_aln_result* out) {
         out->cigars = nullptr;
         out->cigar_offsets = nullptr;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Shared overlap-alignment service (continuous batching for the serving loop)
+
+struct NwSvcState {
+    explicit NwSvcState(int device) : ring(device, sizeof(NwJobDev), "rb_align service") {}
+    RingService ring;
+    void* d_scratch = nullptr;  // one scratch slot per resident warp
+    NwSvcArgs args{};
+    uint32_t slots = 0, grid = 0, max_span = 0;
+};
+
+namespace {
+cudaError_t launch_nw_service(cudaStream_t stream, void* user) {
+    const NwSvcState* S = static_cast<const NwSvcState*>(user);
+    nw_service_kernel<<<S->grid, 32 * kWarpsPerBlock, kWarpsPerBlock * kMaxSym * 32 * 8, stream>>>(S->args);
+    return cudaGetLastError();
+}
+}  // namespace
+
+NwService::NwService(int device, uint32_t max_span, size_t scratch_budget, uint32_t ctas_per_sm) : st_(nullptr) {
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    int sm_count = 148;
+    check_cuda(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
+    std::unique_ptr<NwSvcState> S(new NwSvcState(device));
+    max_span = std::max<uint32_t>(max_span, 64);
+    // the same layout the engine's own kernels use for spans up to max_span
+    const size_t nb = (size_t(max_span) + 63) / 64 + 1, ncols = size_t(max_span) + 64;
+    const size_t stride = warp_scratch_bytes(ncols, nb);
+    size_t warps = size_t(sm_count) * std::max<uint32_t>(1, ctas_per_sm) * kWarpsPerBlock;
+    while (warps > size_t(kWarpsPerBlock) && warps * stride > scratch_budget) warps -= kWarpsPerBlock;
+    S->slots = uint32_t(warps);
+    S->grid = uint32_t(warps / kWarpsPerBlock);
+    S->max_span = max_span;
+    check_cuda(cudaMalloc(&S->d_scratch, warps * stride), "cudaMalloc alignment service scratch");
+    NwSvcArgs& A = S->args;
+    memset(&A, 0, sizeof(A));
+    A.base.scratch = static_cast<uint8_t*>(S->d_scratch);
+    A.base.scratch_stride = stride;
+    A.base.scratch_warps = uint32_t(warps);
+    A.base.max_n = uint32_t(ncols);
+    A.base.max_nb = uint32_t(nb);
+    A.jobs = static_cast<const NwJobDev*>(S->ring.records());
+    A.q = S->ring.queue();
+    check_cuda(cudaFuncSetAttribute(nw_service_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kWarpsPerBlock * kMaxSym * 32 * 8),
+               "cudaFuncSetAttribute");
+    prefer_max_shared(reinterpret_cast<const void*>(nw_service_kernel));
+    st_ = S.release();
+    st_->ring.start(launch_nw_service, st_);
+}
+
+NwService::~NwService() {
+    st_->ring.stop();
+    cudaFree(st_->d_scratch);
+    delete st_;
+}
+
+bool NwService::fits(uint32_t max_m, uint32_t max_n) const {
+    return max_m <= st_->max_span && max_n <= st_->max_span;
+}
+uint32_t NwService::slots() const { return st_->slots; }
+uint32_t NwService::launches() const { return st_->ring.launches(); }
+
+void NwService::run_batch(const NwJobDev& job, const uint32_t* index, size_t n, int queue) {
+    const size_t cap = st_->ring.max_batch();
+    for (size_t b = 0; b < n; b += cap) st_->ring.run_batch(&job, index + b, std::min(cap, n - b), queue);
 }
 
 }  // namespace rb

@@ -34,17 +34,21 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
 #include <cstdlib>
+#include <memory>
 #include <numeric>
 
 #include "rb_internal.hpp"
+#include "ring_queue.cuh"
 
 namespace rb {
 
-// One batch of windows in the shared queue (host-mapped record, written
-// before its items are published): the batch's device buffers, as PoaArgs
-// holds them for a private launch.
+// One batch of windows in the shared queue (device record, written before
+// its items are published): the batch's device buffers, as PoaArgs holds
+// them for a private launch.
 struct PoaJobDev {
+    SvcJobHead head;            // windows of the batch, generation
     const uint8_t* in;
     const PoaWinDev* wins;
     const PoaLayerDev* layers;
@@ -52,9 +56,7 @@ struct PoaJobDev {
     uint32_t* out_len;
     uint8_t* flags;
     unsigned long long* cells;  // [0] DP cells, [1] edge-cells (device)
-    uint32_t total;             // windows of the batch
     int trim;
-    uint32_t generation;        // written to the finished flag when the batch is done
     uint32_t pad;
 };
 
@@ -367,25 +369,6 @@ __device__ bool g_mark_subgraph(const Graph& g, PoaShared& sh, int begin_node, i
 
 __device__ int layer_weight(const uint8_t* qual, int k) { return qual ? int(qual[k]) - 33 : 1; }
 
-// Rank extent, in the incremental order, of the aligned group of an existing
-// node v among the nodes that existed before this insertion (ids < nold).
-__device__ int group_end_rank(const Graph& g, int v, int nold) {
-    int r = g.my_rank[v];
-    for (int x = g.al_head[v]; x != -1; x = g.a_next[x]) {
-        const int y = g.a_node[x];
-        if (y < nold) r = max(r, g.my_rank[y]);
-    }
-    return r;
-}
-__device__ int group_start_rank(const Graph& g, int v, int nold) {
-    int r = g.my_rank[v];
-    for (int x = g.al_head[v]; x != -1; x = g.a_next[x]) {
-        const int y = g.a_node[x];
-        if (y < nold) r = min(r, g.my_rank[y]);
-    }
-    return r;
-}
-
 // Warp prefix helpers: exclusive prefix of v over lanes, and the total.
 __device__ __forceinline__ int warp_excl(int v, int lane, int& total) {
     int x = v;
@@ -520,7 +503,8 @@ __device__ void add_alignment_warp(const Graph& g, PoaShared& sh, const uint8_t*
             if (t >= m) continue;
             int kind = 1, nid = -1, nal = 0, slot = INT_MIN, start = INT_MAX;
             if (at[u] != -1) {
-                // the group's rank extent (group_end_rank / group_start_rank)
+                // the rank extent, in the incremental order, of v's aligned
+                // group among the nodes that existed before this insertion
                 slot = start = rk[u];
                 const bool same = cd[u] == int(letter[u]);
                 for (int x = ah[u]; x != -1; x = g.a_next[x]) {
@@ -2436,76 +2420,13 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kCtasPerSm) poa_plain_kerne
 
 // ---------------- shared queue (serving) ----------------
 
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Priority rings of the shared queue, drained in order: batches go to ring
-// q by size (ring 0 the smallest), so short jobs start first.
-constexpr int kSvcQueues = 4;
-
-// Queue state lives in device memory: the host writes job records, then
-// items, then the tail with copies in one stream (each copy starts after the
-// previous one completes), so a warp that sees the new tail in L2 finds the
-// items and records there too. Idle warps poll that L2 word, never host
-// memory: polling over the bus, or acquire loads at system scope, would slow
-// the warps still computing on the same SMs.
+// The consensus service's kernel arguments: scoring, capacities and scratch
+// slots, the batch records, and the queue.
 struct PoaSvcArgs {
-    PoaArgs base;                    // scoring, capacities, scratch slots
-    const PoaJobDev* jobs;           // device: job records
-    const uint2* items;              // device rings, kSvcQueues x ring_mask + 1 (job slot, window); ring 0 first
-    const unsigned long long* tail;  // device: [kSvcQueues] items published
-    unsigned long long* head;        // device: [kSvcQueues] items claimed
-    unsigned int* live;              // device: [0] warps working on a window, [1] closing (per launch)
-    unsigned long long ring_mask;
-    unsigned int* done;              // device: windows finished per job slot
-    volatile unsigned int* finished; // mapped host: generation of the last finished batch per slot
-    const unsigned int* stop;        // device: leave now
-    unsigned long long idle_ns;      // a warp leaves after this long without work
+    PoaArgs base;
+    const PoaJobDev* jobs;
+    SvcQueueDev q;
 };
-
-// Claims the next item, ring 0 (smallest jobs) first: returns (job << 32) |
-// window, or ~0 when the kernel closes or stop is set. The kernel closes as a
-// whole: a warp that has found no work for idle_ns while no warp of the
-// kernel is working sets the closing word, and every warp leaves at its next
-// poll. (Warps that left one by one would leave work arriving later to the
-// few still busy.) Bounded: once no window is in flight, the kernel ends
-// within idle_ns plus one poll. Out of line with scalar arguments, so its
-// registers do not add to the window code's.
-__device__ __noinline__ unsigned long long svc_claim(const uint2* items,
-                                                     const unsigned long long* tail, unsigned long long* head,
-                                                     unsigned int* live, unsigned long long ring_mask,
-                                                     const unsigned int* stop, unsigned long long idle_ns) {
-    const unsigned long long t0 = global_ns();
-    unsigned int nap = 512;
-    volatile unsigned int* vlive = live;
-    for (;;) {
-        if (*reinterpret_cast<const volatile unsigned int*>(stop) || vlive[1]) return ~0ull;
-        for (int q = 0; q < kSvcQueues; ++q) {
-            const unsigned long long t = reinterpret_cast<const volatile unsigned long long*>(tail)[q];
-            unsigned long long h = reinterpret_cast<volatile unsigned long long*>(head)[q];
-            while (h < t) {
-                const unsigned long long prev = atomicCAS(head + q, h, h + 1);
-                if (prev == h) {
-                    atomicAdd(live, 1u);
-                    __threadfence();
-                    const volatile unsigned int* it = reinterpret_cast<const volatile unsigned int*>(
-                        items + size_t(q) * (ring_mask + 1) + (h & ring_mask));
-                    return (static_cast<unsigned long long>(it[0]) << 32) | it[1];
-                }
-                h = prev;
-            }
-        }
-        if (global_ns() - t0 > idle_ns && vlive[0] == 0) {
-            atomicExch(live + 1, 1u);
-            return ~0ull;
-        }
-        __nanosleep(nap);
-        nap = nap < 32768 ? nap * 2 : nap;
-    }
-}
 
 // Persistent consensus over the shared queue: each warp owns one scratch
 // slot and takes windows of any job until the queue stays empty. Sized for
@@ -2525,8 +2446,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
     __syncwarp();
     for (;;) {
         unsigned long long it = 0;
-        if (lane == 0)
-            it = svc_claim(s.items, s.tail, s.head, s.live, s.ring_mask, s.stop, s.idle_ns);
+        if (lane == 0) it = svc_claim(s.q);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it == ~0ull) break;
         const uint32_t job = uint32_t(it >> 32), win = uint32_t(it);
@@ -2544,8 +2464,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
             a.flags = const_cast<uint8_t*>(J.flags);
             a.trim = J.trim;
             a.cells = const_cast<unsigned long long*>(J.cells);
-            total = J.total;
-            gen = J.generation;
+            total = J.head.total;
+            gen = J.head.generation;
             a.nwin = total;
             a_all[wid] = a;
         }
@@ -2553,14 +2473,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
         poa_window(a_all[wid], g_all[wid], sh, win, lane, ring);
         __threadfence();
         __syncwarp();
-        if (lane == 0) {
-            const unsigned int d = atomicAdd(&s.done[job], 1u) + 1u;
-            if (d == total) {
-                __threadfence_system();
-                s.finished[job] = gen;
-            }
-            atomicSub(s.live, 1u);
-        }
+        if (lane == 0) svc_item_done(s.q, job, total, gen);
     }
 }
 
@@ -2972,95 +2885,45 @@ void PoaEngine::fetch(rb_poa_result* out) {
 // ---------------------------------------------------------------------------
 // Shared window-consensus service (continuous batching for the serving loop)
 
-#include <atomic>
-#include <chrono>
-#include <condition_variable>
-#include <mutex>
-#include <thread>
-
 namespace rb {
 
-namespace {
-constexpr uint32_t kSvcJobs = 256;                  // concurrent batches
-constexpr unsigned long long kSvcRing = 1ull << 21; // items per ring
-// control words (8-byte units): tails, heads, stop, live/closing
-constexpr int kCtlTail = 0, kCtlHead = kSvcQueues, kCtlStop = 2 * kSvcQueues, kCtlLive = 2 * kSvcQueues + 1;
-constexpr size_t kCtlBytes = 128;
-}  // namespace
-
 struct PoaSvcState {
-    int device = 0;
-    DeviceInfo dev;
-    cudaStream_t stream = nullptr;     // the persistent kernel's stream
-    cudaStream_t ctl = nullptr;        // queue writes and head reads (ordered copies)
-    cudaEvent_t done_ev = nullptr;
+    explicit PoaSvcState(int device) : ring(device, sizeof(PoaJobDev), "rb_poa service") {}
+    RingService ring;
+    void* d_scratch = nullptr;  // one graph slot per resident warp
     PoaSvcArgs args{};
-    // device: scratch slots, queue rings, [tail0, tail1, head0, head1, stop],
-    // job records, per-job done counters
-    void* d_scratch = nullptr;
-    uint2* d_items = nullptr;  // kSvcQueues rings of kSvcRing items
-    unsigned long long* d_ctl = nullptr;
-    PoaJobDev* d_jobs = nullptr;
-    unsigned int* d_done = nullptr;
-    // host: pinned staging for the copies, mapped finished flags
-    uint2* h_stage = nullptr;               // kSvcRing / 2 items
-    PoaJobDev* h_rec = nullptr;             // one record
-    unsigned long long* h_val = nullptr;    // tail / stop values
-    unsigned int* h_finished = nullptr;     // [kSvcJobs], mapped
     uint32_t slots = 0, grid = 0;
-    std::mutex mu;       // queue state, dispatcher
-    std::mutex pub_mu;   // publishing (staging buffers and the control stream)
-    std::condition_variable cv, cv_slot;
-    std::vector<uint32_t> free_jobs;
-    std::vector<uint32_t> generation;
-    unsigned long long published[kSvcQueues] = {0, 0, 0, 0};
-    unsigned long long active_items = 0;
-    bool running = false, stopping = false;
-    std::string error;
-    uint32_t launches = 0;
-    std::thread thread;
 };
+
+namespace {
+cudaError_t launch_poa_service(cudaStream_t stream, void* user) {
+    const PoaSvcState* S = static_cast<const PoaSvcState*>(user);
+    poa_service_kernel<<<S->grid, 32 * kWarpsPerCta, kWarpsPerCta * kRingBytesPerWarp, stream>>>(S->args);
+    return cudaGetLastError();
+}
+}  // namespace
 
 PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window_length, size_t scratch_budget,
                        uint32_t ctas_per_sm)
-    : st_(new PoaSvcState()) {
-    PoaSvcState& S = *st_;
-    S.device = device;
+    : st_(nullptr) {
     check_cuda(cudaSetDevice(device), "cudaSetDevice");
-    S.dev.device = device;
-    check_cuda(cudaDeviceGetAttribute(&S.dev.sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
-    check_cuda(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    check_cuda(cudaStreamCreateWithFlags(&S.ctl, cudaStreamNonBlocking), "cudaStreamCreate");
-    check_cuda(cudaEventCreateWithFlags(&S.done_ev, cudaEventDisableTiming), "cudaEventCreate");
+    int sm_count = 148;
+    check_cuda(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
+    std::unique_ptr<PoaSvcState> S(new PoaSvcState(device));
     // slot layout for layers up to three window lengths; longer ones (and
     // graphs over 4096 nodes) overflow and run again in the job's own engine
     const int ncap = 4096, ecap = 2 * ncap, acap = ncap;
     const int lcap = row_cover(int(std::max<uint32_t>(window_length, 1)) * 3 + 1);
     const size_t slot = walk_layout(ncap, ecap, acap, lcap, [](int, size_t) {});
     const uint32_t cps = std::max<uint32_t>(1, std::min<uint32_t>(ctas_per_sm, kSvcCtasPerSm));
-    size_t slots = size_t(S.dev.sm_count) * cps * kWarpsPerCta;
+    size_t slots = size_t(sm_count) * cps * kWarpsPerCta;
     while (slots > kWarpsPerCta && slots * slot > scratch_budget) slots -= kWarpsPerCta;
-    S.slots = uint32_t(slots);
-    S.grid = uint32_t(slots / kWarpsPerCta);
-    check_cuda(cudaMalloc(&S.d_scratch, slots * slot), "cudaMalloc service scratch");
-    check_cuda(cudaMalloc(&S.d_items, sizeof(uint2) * kSvcRing * kSvcQueues), "cudaMalloc service queue");
-    check_cuda(cudaMalloc(&S.d_ctl, kCtlBytes), "cudaMalloc");
-    check_cuda(cudaMalloc(&S.d_jobs, sizeof(PoaJobDev) * kSvcJobs), "cudaMalloc");
-    check_cuda(cudaMalloc(&S.d_done, kSvcJobs * 4), "cudaMalloc");
-    check_cuda(cudaMemset(S.d_ctl, 0, kCtlBytes), "cudaMemset");
-    check_cuda(cudaMemset(S.d_done, 0, kSvcJobs * 4), "cudaMemset");
-    check_cuda(cudaMemset(S.d_jobs, 0, sizeof(PoaJobDev) * kSvcJobs), "cudaMemset");
-    check_cuda(cudaMallocHost(&S.h_stage, sizeof(uint2) * (kSvcRing / 2)), "cudaMallocHost");
-    check_cuda(cudaMallocHost(&S.h_rec, sizeof(PoaJobDev)), "cudaMallocHost");
-    check_cuda(cudaMallocHost(&S.h_val, kCtlBytes), "cudaMallocHost");
-    check_cuda(cudaHostAlloc(&S.h_finished, 4 * kSvcJobs, cudaHostAllocMapped | cudaHostAllocPortable),
-               "cudaHostAlloc mapped");
-    memset(S.h_finished, 0, 4 * kSvcJobs);
-    void* d_fin = nullptr;
-    check_cuda(cudaHostGetDevicePointer(&d_fin, S.h_finished, 0), "cudaHostGetDevicePointer");
-    PoaSvcArgs& A = S.args;
+    S->slots = uint32_t(slots);
+    S->grid = uint32_t(slots / kWarpsPerCta);
+    check_cuda(cudaMalloc(&S->d_scratch, slots * slot), "cudaMalloc service scratch");
+    PoaSvcArgs& A = S->args;
     memset(&A, 0, sizeof(A));
-    A.base.scratch = static_cast<uint8_t*>(S.d_scratch);
+    A.base.scratch = static_cast<uint8_t*>(S->d_scratch);
     A.base.slot_bytes = slot;
     A.base.ncap = ncap;
     A.base.ecap = ecap;
@@ -3069,192 +2932,27 @@ PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window
     A.base.match = m;
     A.base.mismatch = x;
     A.base.gap = g;
-    A.jobs = S.d_jobs;
-    A.items = S.d_items;
-    A.tail = S.d_ctl + kCtlTail;
-    A.head = S.d_ctl + kCtlHead;
-    A.stop = reinterpret_cast<const unsigned int*>(S.d_ctl + kCtlStop);
-    A.live = reinterpret_cast<unsigned int*>(S.d_ctl + kCtlLive);
-    A.ring_mask = kSvcRing - 1;
-    A.done = S.d_done;
-    A.finished = static_cast<unsigned int*>(d_fin);
-    A.idle_ns = 3000000ull;  // 3 ms
-    for (uint32_t j = kSvcJobs; j-- > 0;) S.free_jobs.push_back(j);
-    S.generation.assign(kSvcJobs, 0);
+    A.jobs = static_cast<const PoaJobDev*>(S->ring.records());
+    A.q = S->ring.queue();
     check_cuda(cudaFuncSetAttribute(poa_service_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     kWarpsPerCta * kRingBytesPerWarp),
                "cudaFuncSetAttribute");
     prefer_max_shared(reinterpret_cast<const void*>(poa_service_kernel));
-    keep_pool_reserve(device);
-    S.thread = std::thread([this] { dispatcher(); });
+    st_ = S.release();
+    st_->ring.start(launch_poa_service, st_);
 }
 
 PoaService::~PoaService() {
-    PoaSvcState& S = *st_;
-    {
-        std::lock_guard<std::mutex> lk(S.mu);
-        S.stopping = true;
-    }
-    S.cv.notify_all();
-    S.cv_slot.notify_all();
-    if (S.thread.joinable()) S.thread.join();
-    cudaSetDevice(S.device);
-    {
-        // the stop word ends a running kernel within its idle bound
-        std::lock_guard<std::mutex> lk(S.pub_mu);
-        S.h_val[kCtlStop] = 1;
-        cudaMemcpyAsync(S.d_ctl + kCtlStop, S.h_val + kCtlStop, 8, cudaMemcpyHostToDevice, S.ctl);
-        cudaStreamSynchronize(S.ctl);
-    }
-    cudaStreamSynchronize(S.stream);
-    cudaFree(S.d_scratch);
-    cudaFree(S.d_items);
-    cudaFree(S.d_ctl);
-    cudaFree(S.d_jobs);
-    cudaFree(S.d_done);
-    cudaFreeHost(S.h_stage);
-    cudaFreeHost(S.h_rec);
-    cudaFreeHost(S.h_val);
-    cudaFreeHost(S.h_finished);
-    cudaEventDestroy(S.done_ev);
-    cudaStreamDestroy(S.stream);
-    cudaStreamDestroy(S.ctl);
+    st_->ring.stop();
+    cudaFree(st_->d_scratch);
     delete st_;
 }
 
 uint32_t PoaService::slots() const { return st_->slots; }
-uint32_t PoaService::launches() const { return st_->launches; }
-
-// Keeps the persistent kernel running while items are pending: after the
-// kernel leaves (idle, or racing a publish), items still unclaimed start a
-// new launch.
-void PoaService::dispatcher() {
-    PoaSvcState& S = *st_;
-    cudaSetDevice(S.device);
-    std::unique_lock<std::mutex> lk(S.mu);
-    while (!S.stopping) {
-        S.cv.wait_for(lk, std::chrono::microseconds(500));
-        if (S.stopping) break;
-        if (S.running) {
-            const cudaError_t q = cudaEventQuery(S.done_ev);
-            if (q == cudaErrorNotReady) continue;
-            S.running = false;
-            if (q != cudaSuccess) {
-                S.error = std::string("rb_poa service kernel: ") + cudaGetErrorString(q);
-                S.cv_slot.notify_all();
-                continue;
-            }
-        }
-        if (!S.error.empty()) continue;
-        bool pending = false;
-        {
-            // lock order: mu, then pub_mu (publishers take pub_mu alone)
-            std::lock_guard<std::mutex> plk(S.pub_mu);
-            unsigned long long any = 0;
-            for (int q = 0; q < kSvcQueues; ++q) any += S.published[q];
-            if (any == 0) continue;
-            if (cudaMemcpyAsync(S.h_val + kCtlHead, S.d_ctl + kCtlHead, 8 * kSvcQueues, cudaMemcpyDeviceToHost,
-                                S.ctl) != cudaSuccess ||
-                cudaStreamSynchronize(S.ctl) != cudaSuccess) {
-                S.error = "rb_poa service: head read failed";
-                S.cv_slot.notify_all();
-                continue;
-            }
-            for (int q = 0; q < kSvcQueues; ++q) pending |= S.h_val[kCtlHead + q] < S.published[q];
-        }
-        if (!pending) continue;
-        // a launch starts with no warp working and not closing
-        cudaError_t e = cudaMemsetAsync(S.d_ctl + kCtlLive, 0, 8, S.stream);
-        if (e == cudaSuccess)
-            poa_service_kernel<<<S.grid, 32 * kWarpsPerCta, kWarpsPerCta * kRingBytesPerWarp, S.stream>>>(S.args);
-        if (e == cudaSuccess) e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaEventRecord(S.done_ev, S.stream);
-        if (e != cudaSuccess) {
-            S.error = std::string("rb_poa service launch: ") + cudaGetErrorString(e);
-            S.cv_slot.notify_all();
-            continue;
-        }
-        S.running = true;
-        ++S.launches;
-    }
-}
+uint32_t PoaService::launches() const { return st_->ring.launches(); }
 
 void PoaService::run_batch(const PoaJobDev& job, const uint32_t* order, size_t n, int queue) {
-    PoaSvcState& S = *st_;
-    if (n == 0) return;
-    if (n > kSvcRing / 2) throw Error{RB_ERR_ARG, "rb_poa service: batch larger than the shared queue"};
-    if (queue < 0 || queue >= kSvcQueues) throw Error{RB_ERR_ARG, "rb_poa service: bad queue"};
-    uint32_t slot = 0, gen = 0;
-    {
-        std::unique_lock<std::mutex> lk(S.mu);
-        // a job slot, and room in the rings for every item not yet finished
-        S.cv_slot.wait(lk, [&] {
-            return !S.error.empty() || S.stopping ||
-                   (!S.free_jobs.empty() && S.active_items + n <= kSvcRing / 2);
-        });
-        if (!S.error.empty()) throw Error{RB_ERR_DEVICE, S.error};
-        if (S.stopping) throw Error{RB_ERR_ARG, "rb_poa service: shutting down"};
-        slot = S.free_jobs.back();
-        S.free_jobs.pop_back();
-        S.active_items += n;
-        gen = ++S.generation[slot];
-    }
-    {
-        // record, items, then tail, in one stream: the slot's done counter
-        // starts from zero and its record is in place before any item is
-        // visible, and the items before the tail
-        std::lock_guard<std::mutex> plk(S.pub_mu);
-        const int q = queue;
-        const unsigned long long t = S.published[q];
-        PoaJobDev rec = job;
-        rec.total = uint32_t(n);
-        rec.generation = gen;
-        *S.h_rec = rec;
-        check_cuda(cudaMemsetAsync(S.d_done + slot, 0, 4, S.ctl), "memset done");
-        check_cuda(cudaMemcpyAsync(S.d_jobs + slot, S.h_rec, sizeof(PoaJobDev), cudaMemcpyHostToDevice, S.ctl),
-                   "H2D job record");
-        for (size_t i = 0; i < n; ++i) S.h_stage[i] = make_uint2(slot, order[i]);
-        const size_t at = size_t(t & (kSvcRing - 1));
-        const size_t first = std::min(n, size_t(kSvcRing) - at);
-        uint2* ring = S.d_items + size_t(q) * kSvcRing;
-        check_cuda(cudaMemcpyAsync(ring + at, S.h_stage, first * sizeof(uint2), cudaMemcpyHostToDevice,
-                                   S.ctl),
-                   "H2D items");
-        if (first < n)
-            check_cuda(cudaMemcpyAsync(ring, S.h_stage + first, (n - first) * sizeof(uint2),
-                                       cudaMemcpyHostToDevice, S.ctl),
-                       "H2D items");
-        S.h_val[kCtlTail + q] = t + n;
-        check_cuda(cudaMemcpyAsync(S.d_ctl + kCtlTail + q, S.h_val + kCtlTail + q, 8, cudaMemcpyHostToDevice, S.ctl),
-                   "H2D tail");
-        check_cuda(cudaStreamSynchronize(S.ctl), "service publish");
-        S.published[q] = t + n;
-    }
-    S.cv.notify_all();
-    // wait for the batch; the dispatcher keeps a kernel running meanwhile
-    volatile unsigned int* fin = S.h_finished + slot;
-    std::string err;
-    for (;;) {
-        if (*fin == gen) break;
-        {
-            std::lock_guard<std::mutex> lk(S.mu);
-            if (!S.error.empty()) {
-                err = S.error;
-                break;
-            }
-        }
-        std::this_thread::sleep_for(std::chrono::microseconds(100));
-    }
-    std::atomic_thread_fence(std::memory_order_acquire);
-    {
-        std::lock_guard<std::mutex> lk(S.mu);
-        if (err.empty()) {
-            S.free_jobs.push_back(slot);
-            S.active_items -= n;
-        }
-    }
-    S.cv_slot.notify_all();
-    if (!err.empty()) throw Error{RB_ERR_DEVICE, err};
+    st_->ring.run_batch(&job, order, n, queue);
 }
 
 void PoaEngine::run_shared(PoaService& svc, uint32_t priority_windows) {

@@ -158,6 +158,9 @@ void ctx_set_poa_service(rb_ctx* ctx, PoaService* svc, uint32_t priority_windows
     ctx->svc = svc;
     ctx->svc_priority_windows = priority_windows;
 }
+void ctx_set_nw_service(rb_ctx* ctx, NwService* svc, uint32_t priority_pairs) {
+    if (ctx && ctx->nw) ctx->nw->set_service(svc, priority_pairs);
+}
 }  // namespace rb
 
 namespace {

@@ -76,6 +76,63 @@ void keep_pool_reserve(int device);
 rb_tuning tuning_get(int device);
 void tuning_set(int device, const rb_tuning& t);
 
+// ----- shared work queue of a persistent kernel (ring_service.cpp) -----
+// Continuous batching for the serving loop. Batches (one job's windows, or
+// one pass of one job's alignments) are appended as (batch slot, index)
+// items to size-class rings in device memory; a persistent kernel's warps
+// claim items from the rings (ring 0 first) and report each one done; the
+// last item of a batch raises the batch's flag in mapped host memory. The
+// kernel leaves, as a whole, after a bounded idle time, and a dispatcher
+// thread relaunches it while items are pending.
+constexpr int kSvcQueues = 4;
+
+// Every batch record starts with this header (filled in by run_batch).
+struct SvcJobHead {
+    uint32_t total;       // items in the batch
+    uint32_t generation;  // value the last item writes to the batch's flag
+};
+
+// What the persistent kernel reads and writes (device pointers).
+struct SvcQueueDev {
+    const uint2* items;              // kSvcQueues rings of ring_mask + 1 items, ring 0 first
+    const unsigned long long* tail;  // [kSvcQueues] items published
+    unsigned long long* head;        // [kSvcQueues] items claimed
+    unsigned int* live;              // [0] warps working on an item, [1] closing (per launch)
+    unsigned long long ring_mask;
+    unsigned int* done;              // items finished per batch slot
+    volatile unsigned int* finished; // mapped host: generation of the last finished batch per slot
+    const unsigned int* stop;        // leave now
+    unsigned long long idle_ns;      // the kernel leaves after this long without work
+};
+
+struct RingState;
+
+class RingService {
+public:
+    // record_bytes: size of one batch record (starting with SvcJobHead);
+    // name prefixes error messages.
+    RingService(int device, size_t record_bytes, const char* name);
+    ~RingService();
+    RingService(const RingService&) = delete;
+    RingService& operator=(const RingService&) = delete;
+    // Starts the dispatcher; launch(stream) enqueues one persistent launch.
+    void start(cudaError_t (*launch)(cudaStream_t, void*), void* user);
+    // Ends a running kernel (stop word) and the dispatcher; idempotent.
+    void stop();
+    const SvcQueueDev& queue() const;
+    void* records() const;  // device: one record per batch slot
+    // Appends index[0..n) of the batch described by `record` to ring
+    // `queue` and waits until every item is done. At most max_batch() items.
+    // Throws rb::Error on device failure.
+    void run_batch(const void* record, const uint32_t* index, size_t n, int queue);
+    size_t max_batch() const;
+    uint32_t launches() const;
+
+private:
+    void dispatcher();
+    RingState* st_;
+};
+
 // ----- device sequence store (layers.cu) -----
 // One entry of the staged sequence table: offsets of the forward bases and
 // quality and of the reverse complement and reversed quality in the store.
@@ -105,6 +162,8 @@ struct NwPairDev {
     uint32_t q_offset, t_begin;
 };
 
+class NwService;
+
 class NwEngine {
 public:
     explicit NwEngine(const DeviceInfo& dev, cudaStream_t stream);
@@ -113,7 +172,16 @@ public:
     // Pairs cut from the staged sequence table and encoded on the device.
     void stage_store(const rb_store_pair* pairs, size_t n, int want_cigar, uint32_t window_length,
                      const SeqStore& st);
+    // Aligns the staged pairs: through the shared service when one is set
+    // and the pairs fit its scratch, else on this engine's own kernels.
     void run();
+    // Routes run() through a shared alignment service (nullptr: own
+    // kernels). Batches of at most priority_pairs pairs use the first ring,
+    // larger ones later rings (x4 per ring).
+    void set_service(NwService* svc, uint32_t priority_pairs) {
+        svc_ = svc;
+        svc_priority_ = priority_pairs;
+    }
     void fetch(rb_aln_result* out);
     // Breaking points of the last run on the device: pair i's (t, q) values
     // at bp_slots()[pairs()[i].bp_off ...], bp_counts()[i] of them.
@@ -135,6 +203,11 @@ public:
 
 private:
     void reserve_scratch(uint32_t max_m, uint32_t max_n);
+    void run_own();
+    void run_shared();
+    void finish_outputs(const void* args);
+    NwService* svc_ = nullptr;
+    uint32_t svc_priority_ = 0;
     DeviceInfo dev_;
     cudaStream_t stream_;
     cudaEvent_t ev0_, ev1_, ev2_, ev3_;
@@ -249,19 +322,17 @@ private:
 };
 
 // ----- shared window-consensus service (poa_consensus.cu) -----
-// Continuous batching for the serving loop: one persistent consensus kernel
-// per device whose warps pull (job, window) items from size-class rings in
-// device memory (smallest jobs first), so windows of jobs admitted while
-// others run start as soon as any warp frees up. Jobs append their items and wait for a
-// per-job completion flag; the kernel leaves after a bounded idle time and a
-// dispatcher thread relaunches it when items are pending. Thread-safe.
+// One persistent consensus kernel per device on a RingService: its warps
+// take (job, window) items of every job in flight, smallest jobs' ring
+// first, so windows of jobs admitted while others run start as soon as any
+// warp frees up. Thread-safe.
 struct PoaJobDev;
 struct PoaSvcState;
 
 class PoaService {
 public:
     // ctas_per_sm: resident consensus CTAs (4 warps each) per SM, 1..3; the
-    // rest of the SM stays free for other kernels (alignment of new jobs).
+    // rest of the SM stays free for other kernels.
     PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window_length, size_t scratch_budget,
                uint32_t ctas_per_sm);
     ~PoaService();
@@ -275,8 +346,36 @@ public:
     uint32_t launches() const;
 
 private:
-    void dispatcher();
     PoaSvcState* st_;
+};
+
+// ----- shared overlap-alignment service (nw_align.cu) -----
+// One persistent alignment kernel per device on a RingService: its warps
+// take the distance passes and the path-recursion tasks of every job in
+// flight, smallest jobs' ring first, so a small job's alignments do not wait
+// for a large job's persistent grid to drain. Thread-safe.
+struct NwJobDev;
+struct NwSvcState;
+
+class NwService {
+public:
+    // max_span: longest query and target span a batch may hold (the warps'
+    // scratch is sized for it; longer batches run on the engine's own
+    // kernels); ctas_per_sm: resident alignment CTAs (4 warps each) per SM.
+    NwService(int device, uint32_t max_span, size_t scratch_budget, uint32_t ctas_per_sm);
+    ~NwService();
+    NwService(const NwService&) = delete;
+    NwService& operator=(const NwService&) = delete;
+    bool fits(uint32_t max_m, uint32_t max_n) const;
+    // Enqueues items index[0..n) of `job` (pairs of a distance pass, or
+    // tasks of one recursion level) on ring `queue` and waits for them;
+    // batches above the ring's limit go in parts.
+    void run_batch(const NwJobDev& job, const uint32_t* index, size_t n, int queue);
+    uint32_t slots() const;
+    uint32_t launches() const;
+
+private:
+    NwSvcState* st_;
 };
 
 // ----- device layer assembly (layers.cu) -----
@@ -342,5 +441,8 @@ void ctx_set_poa_budget(rb_ctx* ctx, size_t bytes);
 // (nullptr: its own kernel); batches of at most priority_windows windows use
 // the high-priority queue. Defined in rb_capi.cpp.
 void ctx_set_poa_service(rb_ctx* ctx, PoaService* svc, uint32_t priority_windows);
+// Routes the context's alignments through a shared alignment service
+// (nullptr: its own kernels). Defined in rb_capi.cpp.
+void ctx_set_nw_service(rb_ctx* ctx, NwService* svc, uint32_t priority_pairs);
 
 }  // namespace rb

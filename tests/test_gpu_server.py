@@ -1,7 +1,8 @@
 """Serving loop (rb_server_*): every job's FASTA is the same alone and in the
-mix (with the shared consensus kernel, jobs admitted while it runs; and with
-per-job kernels), admission by footprint serialises jobs under a small
-budget, and a bad job fails alone without stopping the server."""
+mix (with the shared consensus and alignment kernels, jobs admitted while
+they run; with per-job kernels; and with jobs whose spans exceed the shared
+alignment kernel's scratch), admission by footprint serialises jobs under a
+small budget, and a bad job fails alone without stopping the server."""
 import time
 
 import pytest
@@ -91,3 +92,32 @@ def test_server_private_kernels_match(native_lib):
         tickets = [srv.submit(lambda_path(r), lambda_path(o), lambda_path(TARGET)) for r, o in JOBS]
         got = [srv.wait(x)[0] for x in tickets]
     assert got == want
+
+
+def test_server_private_alignment_match(native_lib):
+    """shared_alignment=False: each job aligns on its own kernels; same
+    outputs."""
+    want = _alone(native_lib)
+    with native_lib.Server(0, workers=3, match=5, mismatch=-4, gap=-8, shared_alignment=False) as srv:
+        tickets = [srv.submit(lambda_path(r), lambda_path(o), lambda_path(TARGET)) for r, o in JOBS]
+        got = [srv.wait(x)[0] for x in tickets]
+    assert got == want
+
+
+def test_server_alignment_span_fallback(native_lib, tmp_path):
+    """A shared alignment kernel sized for 13 kb spans: the lambda jobs'
+    overlaps (up to 12016 bases) align through the shared queue, several
+    levels of the path recursion deep, and a job with reads up to 30 kb
+    aligns on its own kernels; all outputs unchanged."""
+    from racon_b200 import synthetic
+    shape = dict(synthetic.CONFIGS[0], mean=9_000, sd=5_000, hi=30_000)
+    r, o, t, _ = synthetic.contig(str(tmp_path / "long"), 0, scale=0.5, params=shape)
+    long_alone = native_lib.polish_files(r, o, t, match=5, mismatch=-4, gap=-8)
+    want = _alone(native_lib)
+    with native_lib.Server(0, workers=3, match=5, mismatch=-4, gap=-8, alignment_max_span=13_000,
+                           priority_pairs=16, alignment_ctas_per_sm=2) as srv:
+        tickets = [srv.submit(r, o, t)] + [srv.submit(lambda_path(rr), lambda_path(oo), lambda_path(TARGET))
+                                           for rr, oo in JOBS]
+        got = [srv.wait(x)[0] for x in tickets]
+    assert got[0] == long_alone
+    assert got[1:] == want
