@@ -109,7 +109,8 @@ struct RingState;
 
 class RingService {
 public:
-    // record_bytes: size of one batch record (starting with SvcJobHead);
+    // record_bytes: sizeof the batch record type (starting with
+    // SvcJobHead); the device table records() is an array of that type.
     // name prefixes error messages.
     RingService(int device, size_t record_bytes, const char* name);
     ~RingService();

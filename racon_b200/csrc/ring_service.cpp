@@ -41,8 +41,7 @@ constexpr size_t kCtlBytes = 128;
 
 struct RingState {
     int device = 0;
-    size_t rec_size = 0;   // bytes of a record
-    size_t rec_bytes = 0;  // record stride on the device (16-byte multiple)
+    size_t rec_bytes = 0;  // one record; also the stride of the device table, which the kernel indexes as an array
     std::string name;
     cudaStream_t stream = nullptr;  // the persistent kernel's stream
     cudaStream_t ctl = nullptr;     // queue writes and head reads (ordered copies)
@@ -76,8 +75,7 @@ struct RingState {
 RingService::RingService(int device, size_t record_bytes, const char* name) : st_(new RingState()) {
     RingState& S = *st_;
     S.device = device;
-    S.rec_size = record_bytes;
-    S.rec_bytes = (record_bytes + 15) & ~size_t(15);
+    S.rec_bytes = record_bytes;
     S.name = name;
     check_cuda(cudaSetDevice(device), "cudaSetDevice");
     check_cuda(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -242,7 +240,7 @@ void RingService::run_batch(const void* record, const uint32_t* index, size_t n,
         std::lock_guard<std::mutex> plk(S.pub_mu);
         const int q = queue;
         const unsigned long long t = S.published[q];
-        memcpy(S.h_rec, record, S.rec_size);
+        memcpy(S.h_rec, record, S.rec_bytes);
         SvcJobHead head{uint32_t(n), gen};
         memcpy(S.h_rec, &head, sizeof(head));
         check_cuda(cudaMemsetAsync(S.d_done + slot, 0, 4, S.ctl), "memset done");
