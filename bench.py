@@ -87,6 +87,8 @@ def _args():
                    help="serving: each job launches its own alignment kernels")
     p.add_argument("--alignment-ctas", type=int, default=0,
                    help="serving: CTAs per SM of the shared alignment kernel (0: 1)")
+    p.add_argument("--large-first-every", type=int, default=0,
+                   help="serving: every k-th warp of the shared kernels takes the largest jobs first (0: none)")
     p.add_argument("--alignment-yield", type=int, default=0,
                    help="serving: alignment pairs per warp and launch for large jobs (0: persistent)")
     p.add_argument("--alignment-share", type=int, default=0,
@@ -273,6 +275,7 @@ def run_serving(args, device, rates):
     out["shared_consensus"] = not args.no_shared_consensus
     out["shared_alignment"] = not args.no_shared_alignment
     out["alignment_ctas_per_sm"] = args.alignment_ctas or 1
+    out["large_first_every"] = args.large_first_every
     out["alignment_yield"] = args.alignment_yield
     out["alignment_share"] = args.alignment_share
     t_start = time.perf_counter()
@@ -286,7 +289,8 @@ def run_serving(args, device, rates):
                            alignment_yield=args.alignment_yield,
                            alignment_share=args.alignment_share,
                            shared_alignment=not args.no_shared_alignment,
-                           alignment_ctas_per_sm=args.alignment_ctas) as srv:
+                           alignment_ctas_per_sm=args.alignment_ctas,
+                           large_first_every=args.large_first_every) as srv:
         def run(arrivals):
             t0 = time.perf_counter()
             tickets = []
@@ -309,18 +313,26 @@ def run_serving(args, device, rates):
         for t in [srv.submit(*jobs[big][:3]) for _ in range(args.workers)]:
             srv.wait(t)
         log("workers warmed with the largest job")
+        # each job alone, twice; the faster run is its isolated time
         iso, alone, iso_stage = [], [], []
         for j in jobs:
-            fasta, tm = srv.wait(srv.submit(j[0], j[1], j[2]))
-            alone.append(fasta)
-            iso.append(tm["finished"] - tm["submitted"])
-            iso_stage.append(tm["stage_seconds"])
+            best = None
+            for _ in range(2):
+                fasta, tm = srv.wait(srv.submit(j[0], j[1], j[2]))
+                dt = tm["finished"] - tm["submitted"]
+                if best is None or dt < best[0]:
+                    best = (dt, fasta, list(tm["stage_seconds"]))
+            iso.append(best[0])
+            alone.append(best[1])
+            iso_stage.append(best[2])
         log("isolated runs done, sum %.2f s" % sum(iso))
         fastas, _, span = run(None)
         assert fastas == alone, "a job's output differs between alone and in the mix"
         peak = len(jobs) / span
         log("peak run done, makespan %.2f s" % span)
-        out.update(isolated_s={"p50": _pct(iso, 50), "max": max(iso), "sum": sum(iso)},
+        slow = max(range(len(jobs)), key=lambda k: iso[k])
+        out.update(isolated_s={"p50": _pct(iso, 50), "max": max(iso), "sum": sum(iso),
+                               "max_job": {"windows": windows[slow], "stage_s": iso_stage[slow]}},
                    peak={"jobs_per_s": peak, "windows_per_s": sum(windows) / span, "makespan_s": span})
         sweep = []
         rng = random.Random(4)

@@ -406,7 +406,10 @@ void rb_free(void* p);
  * each level before publishing the next. alignment_ctas_per_sm (0: 1) sizes
  * the kernel (4 warps per CTA). Its scratch is sized for spans up to
  * alignment_max_span bases (0: 131072); a job with a longer query or target
- * span aligns on its own kernels. Results are unchanged either way. */
+ * span aligns on its own kernels. large_first_every = k > 0 makes every k-th
+ * warp of both shared kernels drain the rings largest first, so that the
+ * largest jobs keep a share of the warps under a stream of small ones (0:
+ * strict smallest first). Results are unchanged either way. */
 typedef struct rb_server_params {
     int device;
     uint32_t workers;
@@ -424,6 +427,7 @@ typedef struct rb_server_params {
     uint32_t alignment_ctas_per_sm;
     uint32_t alignment_max_span;
     uint32_t priority_pairs;
+    uint32_t large_first_every;
 } rb_server_params;
 
 /* One job: racon's inputs and per-job flags (-f, -q, -e, --no-trimming, -u). */

@@ -95,7 +95,8 @@ class _ServerParams(ctypes.Structure):
                 ("consensus_ctas_per_sm", ctypes.c_uint32), ("priority_windows", ctypes.c_uint32),
                 ("alignment_yield", ctypes.c_uint32), ("alignment_share", ctypes.c_uint32),
                 ("shared_alignment", ctypes.c_int), ("alignment_ctas_per_sm", ctypes.c_uint32),
-                ("alignment_max_span", ctypes.c_uint32), ("priority_pairs", ctypes.c_uint32)]
+                ("alignment_max_span", ctypes.c_uint32), ("priority_pairs", ctypes.c_uint32),
+                ("large_first_every", ctypes.c_uint32)]
 
 
 class _ServerJob(ctypes.Structure):
@@ -631,17 +632,19 @@ class Server:
     queue (continuous batching); jobs of at most priority_windows windows go
     first. With shared_alignment (the default) one persistent alignment
     kernel does the same for the jobs' overlap alignments (jobs of at most
-    priority_pairs pairs first; spans up to alignment_max_span bases).
-    submit() returns a ticket; wait(ticket) returns (fasta, times)."""
+    priority_pairs pairs first; spans up to alignment_max_span bases). With
+    large_first_every = k, every k-th warp of both kernels takes the largest
+    jobs first. submit() returns a ticket; wait(ticket) returns (fasta, times)."""
 
     def __init__(self, device=0, workers=4, hbm_budget=0, match=3, mismatch=-5, gap=-4, window_length=500,
                  shared_consensus=True, consensus_ctas_per_sm=0, priority_windows=0, alignment_yield=0,
                  alignment_share=0, shared_alignment=True, alignment_ctas_per_sm=0, alignment_max_span=0,
-                 priority_pairs=0):
+                 priority_pairs=0, large_first_every=0):
         self.lib = load()
         p = _ServerParams(device, workers, hbm_budget, match, mismatch, gap, window_length, int(shared_consensus),
                           consensus_ctas_per_sm, priority_windows, alignment_yield, alignment_share,
-                          int(shared_alignment), alignment_ctas_per_sm, alignment_max_span, priority_pairs)
+                          int(shared_alignment), alignment_ctas_per_sm, alignment_max_span, priority_pairs,
+                          large_first_every)
         self.ptr = self.lib.rb_server_create(ctypes.byref(p))
         if not self.ptr:
             msg = self.lib.rb_server_error().decode() or self.lib.rb_create_error().decode()

@@ -202,7 +202,8 @@ rb_server* rb_server_create(const rb_server_params* params) {
         const uint32_t cps = s->params.consensus_ctas_per_sm ? s->params.consensus_ctas_per_sm : 2;
         try {
             s->svc.reset(new rb::PoaService(params->device, params->match, params->mismatch, params->gap,
-                                            params->window_length, s->params.hbm_budget / 2, cps));
+                                            params->window_length, s->params.hbm_budget / 2, cps,
+                                            s->params.large_first_every));
         } catch (const rb::Error& e) {
             for (rb_ctx* x : s->ctxs) rb_destroy(x);
             t_server_error = e.msg;
@@ -219,7 +220,8 @@ rb_server* rb_server_create(const rb_server_params* params) {
         const uint32_t cps = s->params.alignment_ctas_per_sm ? s->params.alignment_ctas_per_sm : 1;
         const uint32_t span = s->params.alignment_max_span ? s->params.alignment_max_span : 131072;
         try {
-            s->nw_svc.reset(new rb::NwService(params->device, span, size_t(4) << 30, cps));
+            s->nw_svc.reset(new rb::NwService(params->device, span, size_t(4) << 30, cps,
+                                              s->params.large_first_every));
         } catch (const rb::Error& e) {
             s->svc.reset();
             for (rb_ctx* x : s->ctxs) rb_destroy(x);

@@ -717,7 +717,7 @@ nw_service_kernel(NwSvcArgs s) {
     const WarpScratch ws = warp_scratch(s.base, slot);
     for (;;) {
         unsigned long long it = 0;
-        if (lane == 0) it = svc_claim(s.q);
+        if (lane == 0) it = svc_claim(s.q, slot);
         it = __shfl_sync(kFull, it, 0);
         if (it == ~0ull) break;
         const uint32_t job = uint32_t(it >> 32), idx = uint32_t(it);
@@ -1795,7 +1795,9 @@ cudaError_t launch_nw_service(cudaStream_t stream, void* user) {
 }
 }  // namespace
 
-NwService::NwService(int device, uint32_t max_span, size_t scratch_budget, uint32_t ctas_per_sm) : st_(nullptr) {
+NwService::NwService(int device, uint32_t max_span, size_t scratch_budget, uint32_t ctas_per_sm,
+                     uint32_t large_first_every)
+    : st_(nullptr) {
     check_cuda(cudaSetDevice(device), "cudaSetDevice");
     int sm_count = 148;
     check_cuda(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "sm count");
@@ -1817,6 +1819,7 @@ NwService::NwService(int device, uint32_t max_span, size_t scratch_budget, uint3
     A.base.scratch_warps = uint32_t(warps);
     A.base.max_n = uint32_t(ncols);
     A.base.max_nb = uint32_t(nb);
+    S->ring.set_large_first_every(large_first_every);
     A.jobs = static_cast<const NwJobDev*>(S->ring.records());
     A.q = S->ring.queue();
     check_cuda(cudaFuncSetAttribute(nw_service_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -2446,7 +2446,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, kSvcCtasPerSm) poa_service_
     __syncwarp();
     for (;;) {
         unsigned long long it = 0;
-        if (lane == 0) it = svc_claim(s.q);
+        if (lane == 0) it = svc_claim(s.q, slot);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it == ~0ull) break;
         const uint32_t job = uint32_t(it >> 32), win = uint32_t(it);
@@ -2904,7 +2904,7 @@ cudaError_t launch_poa_service(cudaStream_t stream, void* user) {
 }  // namespace
 
 PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window_length, size_t scratch_budget,
-                       uint32_t ctas_per_sm)
+                       uint32_t ctas_per_sm, uint32_t large_first_every)
     : st_(nullptr) {
     check_cuda(cudaSetDevice(device), "cudaSetDevice");
     int sm_count = 148;
@@ -2932,6 +2932,7 @@ PoaService::PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window
     A.base.match = m;
     A.base.mismatch = x;
     A.base.gap = g;
+    S->ring.set_large_first_every(large_first_every);
     A.jobs = static_cast<const PoaJobDev*>(S->ring.records());
     A.q = S->ring.queue();
     check_cuda(cudaFuncSetAttribute(poa_service_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -103,6 +103,8 @@ struct SvcQueueDev {
     volatile unsigned int* finished; // mapped host: generation of the last finished batch per slot
     const unsigned int* stop;        // leave now
     unsigned long long idle_ns;      // the kernel leaves after this long without work
+    uint32_t large_first_every;      // 0: every warp drains ring 0 first; k: warps k-1, 2k-1, ... drain the last ring first
+    uint32_t pad;
 };
 
 struct RingState;
@@ -116,6 +118,10 @@ public:
     ~RingService();
     RingService(const RingService&) = delete;
     RingService& operator=(const RingService&) = delete;
+    // Every k-th warp drains the rings largest first (0: none), so the
+    // largest jobs keep a share of the warps under a stream of small ones.
+    // Set before start().
+    void set_large_first_every(uint32_t k);
     // Starts the dispatcher; launch(stream) enqueues one persistent launch.
     void start(cudaError_t (*launch)(cudaStream_t, void*), void* user);
     // Ends a running kernel (stop word) and the dispatcher; idempotent.
@@ -334,8 +340,9 @@ class PoaService {
 public:
     // ctas_per_sm: resident consensus CTAs (4 warps each) per SM, 1..3; the
     // rest of the SM stays free for other kernels.
+    // large_first_every: RingService::set_large_first_every.
     PoaService(int device, int8_t m, int8_t x, int8_t g, uint32_t window_length, size_t scratch_budget,
-               uint32_t ctas_per_sm);
+               uint32_t ctas_per_sm, uint32_t large_first_every = 0);
     ~PoaService();
     PoaService(const PoaService&) = delete;
     PoaService& operator=(const PoaService&) = delete;
@@ -363,7 +370,8 @@ public:
     // max_span: longest query and target span a batch may hold (the warps'
     // scratch is sized for it; longer batches run on the engine's own
     // kernels); ctas_per_sm: resident alignment CTAs (4 warps each) per SM.
-    NwService(int device, uint32_t max_span, size_t scratch_budget, uint32_t ctas_per_sm);
+    NwService(int device, uint32_t max_span, size_t scratch_budget, uint32_t ctas_per_sm,
+              uint32_t large_first_every = 0);
     ~NwService();
     NwService(const NwService&) = delete;
     NwService& operator=(const NwService&) = delete;

@@ -21,24 +21,25 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// Claims the next item, ring 0 (smallest jobs) first: returns (batch slot <<
-// 32) | index, or ~0 when the kernel closes or stop is set. The kernel
-// closes as a whole: a warp that has found no work for idle_ns while no warp
-// of the kernel is working sets the closing word, and every warp leaves at
-// its next poll. (Warps that left one by one would leave work arriving later
+// Claims the next item, ring 0 (smallest jobs) first, or the last ring
+// first when large_first: returns (batch slot << 32) | index, or ~0 when the
+// kernel closes or stop is set. The kernel closes as a whole: a warp that
+// has found no work for idle_ns while no warp of the kernel is working sets
+// the closing word, and every warp leaves at its next poll. (Warps that left one by one would leave work arriving later
 // to the few still busy.) Bounded: once no item is in flight, the kernel
 // ends within idle_ns plus one poll. Out of line with scalar arguments, so
 // its registers do not add to the item code's. Lane 0 only.
 __device__ __noinline__ unsigned long long svc_claim(const uint2* items, const unsigned long long* tail,
                                                      unsigned long long* head, unsigned int* live,
                                                      unsigned long long ring_mask, const unsigned int* stop,
-                                                     unsigned long long idle_ns) {
+                                                     unsigned long long idle_ns, bool large_first) {
     const unsigned long long t0 = global_ns();
     unsigned int nap = 512;
     volatile unsigned int* vlive = live;
     for (;;) {
         if (*reinterpret_cast<const volatile unsigned int*>(stop) || vlive[1]) return ~0ull;
-        for (int q = 0; q < kSvcQueues; ++q) {
+        for (int k = 0; k < kSvcQueues; ++k) {
+            const int q = large_first ? kSvcQueues - 1 - k : k;
             const unsigned long long t = reinterpret_cast<const volatile unsigned long long*>(tail)[q];
             unsigned long long h = reinterpret_cast<volatile unsigned long long*>(head)[q];
             while (h < t) {
@@ -62,8 +63,10 @@ __device__ __noinline__ unsigned long long svc_claim(const uint2* items, const u
     }
 }
 
-__device__ __forceinline__ unsigned long long svc_claim(const SvcQueueDev& q) {
-    return svc_claim(q.items, q.tail, q.head, q.live, q.ring_mask, q.stop, q.idle_ns);
+// Warp `slot` of the kernel claims its next item.
+__device__ __forceinline__ unsigned long long svc_claim(const SvcQueueDev& q, uint32_t slot) {
+    const bool large_first = q.large_first_every != 0 && slot % q.large_first_every == q.large_first_every - 1;
+    return svc_claim(q.items, q.tail, q.head, q.live, q.ring_mask, q.stop, q.idle_ns, large_first);
 }
 
 // Lane 0, after the item's writes are fenced: counts the item done for its

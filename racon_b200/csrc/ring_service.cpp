@@ -112,6 +112,8 @@ RingService::RingService(int device, size_t record_bytes, const char* name) : st
     keep_pool_reserve(device);
 }
 
+void RingService::set_large_first_every(uint32_t k) { st_->q.large_first_every = k; }
+
 void RingService::start(cudaError_t (*launch)(cudaStream_t, void*), void* user) {
     RingState& S = *st_;
     S.launch = launch;
