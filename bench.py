@@ -28,7 +28,7 @@ untimed; a step is the consensus of every window of the job.
          the same windows with every host thread
   pipeline  the whole job through rb_polish_files against the oracle's
          pipeline on every host thread, FASTA compared byte for byte
-  serving  config-4 jobs through the serving loop (shared consensus kernel)
+  serving  config-4 jobs through the serving loop (shared consensus and alignment kernels)
          at 80 % of its measured peak
 
 --impl reference runs the CPU oracle as the reference arm (rank 0 only).
