@@ -65,6 +65,10 @@ constexpr int kWarpsPerBlock = 4;
 constexpr int kMaxSym = 32;        // symbols whose bit masks fit the shared-memory table
 constexpr int kMaxSymWide = 256;   // any byte alphabet: the masks then live in the warp's scratch
 constexpr long long kLeafBytes = 1024 * 1024;  // edlib's traceback threshold
+// The diagonal sweep (warp_sweep_diag) handles alphabets of up to kDiagSym
+// symbols and bands whose diagonals stay within kDiagBand of the main one.
+constexpr int kDiagSym = 8;
+constexpr int kDiagBand = 1900;
 
 enum NwStatus : int {
     kNwOk = 0,
@@ -165,6 +169,7 @@ struct WarpScratch {
     u64* capr_mv;
     int32_t* capr_sc;
     uint4* leaf;  // followed by the [kMaxSymWide][32] bit masks of pairs with more than kMaxSym symbols
+    u64* block_peq;  // [max_nb][kDiagSym] query masks per block (diagonal sweep); nullptr: strips only
 };
 
 // Bit masks of a wide-alphabet pair: the region after the leaf store.
@@ -192,13 +197,15 @@ __device__ WarpScratch warp_scratch(const NwDevArgs& a, uint32_t slot) {
     w.capr_mv = reinterpret_cast<u64*>(take(nb * 8));
     w.capr_sc = reinterpret_cast<int32_t*>(take(nb * 4));
     w.leaf = reinterpret_cast<uint4*>(take(kLeafBytes));  // kLeafBytes is a multiple of 256
+    take(size_t(kMaxSymWide) * 32 * 8);                     // wide-alphabet masks (peq_wide)
+    w.block_peq = reinterpret_cast<u64*>(take(nb * kDiagSym * 8));
     return w;
 }
 
 size_t warp_scratch_bytes(size_t n, size_t nb) {
     auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
     return 2 * r(n) + 2 * r(n * 4) + 2 * (2 * r(nb * 8) + r(nb * 4)) + r(kLeafBytes) +
-           r(size_t(kMaxSymWide) * 32 * 8);
+           r(size_t(kMaxSymWide) * 32 * 8) + r(nb * kDiagSym * 8);
 }
 
 enum SweepMode { kDistance = 0, kCapture = 1, kLeaf = 2 };
@@ -232,9 +239,143 @@ struct SweepFail {
 // a computed in-band value is at most the cost of any path to it inside the
 // band, so no path of cost <= k crosses row R. (Out-of-band cells only lower
 // the minimum.) The distance of a pass that reaches the end is unchanged.
+// The same sweep as one diagonal wavefront over all blocks, for narrow
+// bands. Block v runs on lane v % 32 and meets column c at step c + v, so
+// each block gets the carry of block v - 1 at the same column from the lane
+// before it at the previous step (lane 31 to lane 0 by a rotating shuffle,
+// no carry buffer), and a lane moves on to block v + 32 when block v leaves
+// the band. A lane's blocks never overlap in steps, and the lane before it
+// is never already on its next block while this one needs the carry, when
+// both band edges stay within kDiagBand (< 1953) diagonals: then no block
+// starts before 2048 - kDiagBand columns past the start of the block 31
+// below it... 32 above it. The steps are about n + m / 64 instead of
+// (m / 2048) * (2048 + k) for strips, and every cell gets the same inputs
+// as in the strip sweep (the carry of the block above at the same column,
+// +1 where that block is outside the band, the block's first score from the
+// block above one column to the left), so every value, the give-up checks
+// and their rows are the strip sweep's. Query masks come from a per-block
+// table built once per sweep (at most kDiagSym symbols).
+__device__ __forceinline__ bool diag_sweep_ok(const SweepIO& io, const Band& B, const WarpScratch& ws) {
+    return ws.block_peq != nullptr && io.nsym <= kDiagSym && B.dhi <= kDiagBand && B.dhi - B.dlo <= kDiagBand;
+}
+
+template <int MODE>
+__device__ int warp_sweep_diag(const SweepIO& io, const Band& B, const WarpScratch& ws, int lane,
+                               SweepFail* fail) {
+    const int m = B.m, n = B.n, nb = B.nb, nsym = io.nsym;
+    const int ncols = io.ncols;
+    // masks of every block (lane v % 32 builds block v, and only it reads
+    // them back), built in the lane's column of the shared table
+    for (int v0 = 0; v0 < nb; v0 += 32) {
+        const int v = v0 + lane;
+        if (v < nb) {
+            for (int sym = 0; sym < nsym; ++sym) io.peq[sym * 32 + lane] = 0ull;
+            const int r0 = 64 * v;
+            const int rows = min(64, m - r0);
+            for (int i = 0; i < rows; ++i) {
+                const int r = r0 + i;
+                const int code = io.rev ? io.q[m - 1 - r] : io.q[r];
+                io.peq[code * 32 + lane] |= (1ull << i);
+            }
+            const u64 pad = rows < 64 ? (~0ull << rows) : 0ull;  // rows past the query end match anything
+            for (int sym = 0; sym < nsym; ++sym) ws.block_peq[v * kDiagSym + sym] = io.peq[sym * 32 + lane] | pad;
+        }
+    }
+    // the last block that meets the swept columns, and the last step; a
+    // distance sweep also runs to the last step of the bottom block of that
+    // block's 32-block group, where the strip sweep checks the group's row
+    const int v_last = min(nb - 1, (ncols - 1 + B.dhi) / 64);
+    auto last_step = [&](int v) { return min(ncols - 1, 64 * v + 63 - B.dlo) + v; };
+    int t_stop = last_step(v_last);
+    const int g_last = 32 * (v_last / 32) + 31;
+    if (MODE == kDistance && g_last < nb - 1) t_stop = max(t_stop, last_step(g_last));
+    int chk_v = 31;                  // next group-bottom block whose row is checked
+    int chk_t = last_step(chk_v);    // ... at the end of this step
+    int result = INT_MAX;
+    int v = lane;
+    int cb_lo = max(0, 64 * v - B.dhi), cb_hi = min(ncols - 1, 64 * v + 63 - B.dlo);
+    const u64* mask = ws.block_peq + v * kDiagSym;
+    u64 pv = 0, mv = 0;
+    int score = 0;
+    bool started = false;
+    int bottom_min = INT_MAX;  // kDistance, lane 31: minimum of its block's bottom row
+    int in_pack = 0;           // previous step of the lane before: (score << 3) | (processed << 2) | (hout + 1)
+    const int src = (lane + 31) & 31;
+    for (int t = 0; t <= t_stop; ++t) {
+        int c = t - v;
+        if (c > cb_hi) {  // the lane's block left the band: its next block
+            v += 32;
+            c -= 32;
+            cb_lo = max(0, 64 * v - B.dhi);
+            cb_hi = min(ncols - 1, 64 * v + 63 - B.dlo);
+            mask = ws.block_peq + v * kDiagSym;
+            started = false;
+            bottom_min = INT_MAX;
+        }
+        const bool active = v < nb && c >= cb_lo && c <= cb_hi;
+        int hout = 0;
+        if (active) {
+            const int up_h = (in_pack & 3) - 1;
+            const bool up_proc = (in_pack >> 2) & 1;
+            const int up_score = in_pack >> 3;
+            const int hin = (v == 0 || !up_proc) ? 1 : up_h;
+            if (!started) {
+                started = true;
+                pv = ~0ull;
+                mv = 0ull;
+                score = c == 0 ? 64 * (v + 1) : (up_proc ? up_score - up_h : up_score) + 64;
+            }
+            const int tc = io.rev ? io.t[n - 1 - c] : io.t[c];
+            const u64 eq = mask[tc];
+            u64 ph;
+            hout = myers_step(pv, mv, eq, hin, ph);
+            score += hout;
+            if (MODE == kLeaf) {
+                const int blo = band_lo_block(B, c);
+                io.leaf[size_t(c) * io.bw + (v - blo)] =
+                    make_uint4(unsigned(pv), unsigned(pv >> 32), unsigned(ph), unsigned(ph >> 32));
+            }
+            if (MODE == kCapture && c == ncols - 1) {
+                io.cap_pv[v] = pv;
+                io.cap_mv[v] = mv;
+                io.cap_sc[v] = score;
+            }
+            if (MODE == kDistance && v == nb - 1 && c == n - 1) {
+                result = block_value(pv, mv, score, (m - 1) & 63);
+            }
+            if (MODE == kDistance && lane == 31) bottom_min = min(bottom_min, score);
+        }
+        const int pack = (score << 3) | ((active ? 1 : 0) << 2) | (hout + 1);
+        in_pack = __shfl_sync(kFull, pack, src);
+        if (MODE == kDistance && t == chk_t) {
+            // the group whose bottom block is chk_v is done (the strip
+            // sweep's check after that strip)
+            if (chk_v < nb - 1) {
+                const int row_min = __shfl_sync(kFull, bottom_min, 31);
+                const int R = 64 * chk_v + 63;
+                if (row_min > B.k && R + 1 > B.k) {
+                    if (fail) {
+                        fail->row = R;
+                        fail->min = row_min;
+                    }
+                    result = INT_MAX;
+                    break;
+                }
+            }
+            chk_v += 32;
+            chk_t = last_step(chk_v);
+        }
+    }
+    if (MODE == kDistance) {
+        for (int o = 16; o > 0; o >>= 1) result = min(result, __shfl_xor_sync(kFull, result, o));
+    }
+    return result;
+}
+
 template <int MODE>
 __device__ int warp_sweep(const SweepIO& io, const Band& B, const WarpScratch& ws, int lane,
                           unsigned int* counters, SweepFail* fail = nullptr) {
+    if (diag_sweep_ok(io, B, ws)) return warp_sweep_diag<MODE>(io, B, ws, lane, fail);
     int result = INT_MAX;
     const int nstrips = (B.nb + 31) / 32;
     const int m = B.m, n = B.n;
@@ -1080,6 +1221,7 @@ __global__ void __launch_bounds__(32) nw_distance_noalloc_kernel(const char* q, 
     ws.capl_pv = ws.capl_mv = ws.capr_pv = ws.capr_mv = nullptr;
     ws.capl_sc = ws.capr_sc = nullptr;
     ws.leaf = nullptr;
+    ws.block_peq = nullptr;  // strip sweeps only
     // symbols present, numbered by byte value (the distance does not depend
     // on the numbering); more than 32 distinct symbols is reported as -1
     for (int c = lane; c < 256; c += 32) present[c] = 0;
