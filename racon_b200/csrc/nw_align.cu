@@ -66,10 +66,9 @@ constexpr int kMaxSym = 32;        // symbols whose bit masks fit the shared-mem
 constexpr int kMaxSymWide = 256;   // any byte alphabet: the masks then live in the warp's scratch
 constexpr long long kLeafBytes = 1024 * 1024;  // edlib's traceback threshold
 // The diagonal sweep (warp_sweep_diag) handles alphabets of up to kDiagSym
-// symbols and bands whose diagonals stay within 2000 x kDiagSlots - 100 of
-// the main one.
+// symbols and bands whose diagonals stay within kDiagBand of the main one.
 constexpr int kDiagSym = 8;
-constexpr int kDiagSlots = 2;  // blocks a lane carries at once (bands up to 2000 x slots - 100)
+constexpr int kDiagBand = 1900;
 
 enum NwStatus : int {
     kNwOk = 0,
@@ -232,40 +231,32 @@ struct SweepFail {
     int min = 0;
 };
 
-// Banded block sweep of one subproblem by one warp. MODE kDistance returns
-// the value of cell (m-1, n-1) (INT_MAX if the band never reached it). It
-// also stops early, returning INT_MAX, once every computed cell of a full
-// strip's bottom row R exceeds k and so does the left boundary (R + 1): costs
-// never fall along a path, every path of cost <= k stays inside the band, and
-// a computed in-band value is at most the cost of any path to it inside the
-// band, so no path of cost <= k crosses row R. (Out-of-band cells only lower
-// the minimum.) The distance of a pass that reaches the end is unchanged.
-// The same sweep as one diagonal wavefront over all blocks. Block v meets
-// column c at step c + v, on lane v % 32, in slot (v / 32) % P of that lane:
-// a lane carries P blocks at once (P independent Myers chains per step),
-// and a slot moves on to block v + 32P when block v leaves the band. Block v
-// gets the carry of block v - 1 at the same column from the lane before at
-// the previous step, same slot (lane 31 to lane 0 by a rotating shuffle,
-// from the slot before: no carry buffer). With both band edges within
-// 2000P - 100 diagonals of the main one, a slot's blocks never overlap in
-// steps and the lane before never holds its next block in that slot while
-// the carry is needed, so every cell gets the strip sweep's inputs (the
-// carry of the block above at the same column, +1 where that block is
-// outside the band, the block's first score from the block above one column
-// to the left): every value, the give-up checks (at the last step of each
-// 32-block group's bottom block) and their rows are the strip sweep's. The
-// steps are about n + m / 64 instead of (m / 2048)(2048 + k + 95). Query
-// masks come from a per-block table built once per sweep (at most kDiagSym
-// symbols).
-__device__ __forceinline__ int diag_slots(const SweepIO& io, const Band& B, const WarpScratch& ws) {
-    if (ws.block_peq == nullptr || io.nsym > kDiagSym) return 0;
-    const int w = max(B.dhi, B.dhi - B.dlo);
-    for (int p = 1; p <= kDiagSlots; ++p)
-        if (w <= 2000 * p - 100) return p;
-    return 0;
+// The banded block sweep below (warp_sweep) as one diagonal wavefront over
+// all blocks instead of strips, for narrow bands. Block v runs on lane
+// v % 32 and meets column c at step c + v, so it gets the carry of block
+// v - 1 at the same column from the lane before at the previous step (lane
+// 31 to lane 0 by a rotating shuffle, no carry buffer), and a lane moves on
+// to block v + 32 when block v leaves the band. With both band edges within
+// kDiagBand (< 1953) diagonals of the main one, block v + 32 starts at least
+// 32 steps after block v ends, and block v + 31 (the next block of the lane
+// before) starts only after the last step at which block v reads its carry,
+// so a lane never holds two blocks at once and the carry it reads is always
+// block v - 1's. The steps are about n + m / 64 instead of
+// (m / 2048) * (2048 + k) for strips, and every cell gets the same inputs
+// as in the strip sweep (the carry of the block above at the same column,
+// +1 where that block is outside the band, the block's first score from the
+// block above one column to the left), so every value, the give-up checks
+// and their rows are the strip sweep's. Query masks come from a per-block
+// table built once per sweep (at most kDiagSym symbols). A form with two
+// blocks in flight per lane (two slots, bands up to 3900 diagonals) gave the
+// same cells but was slower than strips on the config-2 batch (18217
+// against 19101 pairs/s at 20000 pairs): the per-slot bookkeeping outweighs
+// the second chain.
+__device__ __forceinline__ bool diag_sweep_ok(const SweepIO& io, const Band& B, const WarpScratch& ws) {
+    return ws.block_peq != nullptr && io.nsym <= kDiagSym && B.dhi <= kDiagBand && B.dhi - B.dlo <= kDiagBand;
 }
 
-template <int MODE, int P>
+template <int MODE>
 __device__ int warp_sweep_diag(const SweepIO& io, const Band& B, const WarpScratch& ws, int lane,
                                SweepFail* fail) {
     const int m = B.m, n = B.n, nb = B.nb, nsym = io.nsym;
@@ -295,87 +286,69 @@ __device__ int warp_sweep_diag(const SweepIO& io, const Band& B, const WarpScrat
     int t_stop = last_step(v_last);
     const int g_last = 32 * (v_last / 32) + 31;
     if (MODE == kDistance && g_last < nb - 1) t_stop = max(t_stop, last_step(g_last));
-    int chk_v = 31;                // next group-bottom block whose row is checked
-    int chk_t = last_step(chk_v);  // ... at the end of this step
+    int chk_v = 31;                  // next group-bottom block whose row is checked
+    int chk_t = last_step(chk_v);    // ... at the end of this step
     int result = INT_MAX;
-    int v[P], cb_lo[P], cb_hi[P], score[P], bottom_min[P], in_pack[P];
-    u64 pv[P], mv[P];
-    bool started[P];
-#pragma unroll
-    for (int j = 0; j < P; ++j) {
-        v[j] = lane + 32 * j;
-        cb_lo[j] = max(0, 64 * v[j] - B.dhi);
-        cb_hi[j] = min(ncols - 1, 64 * v[j] + 63 - B.dlo);
-        score[j] = 0;
-        bottom_min[j] = INT_MAX;  // kDistance, lane 31: minimum of the slot's block's bottom row
-        in_pack[j] = 0;           // (score << 3) | (processed << 2) | (hout + 1) of block v - 1, previous step
-        pv[j] = mv[j] = 0ull;
-        started[j] = false;
-    }
+    int v = lane;
+    int cb_lo = max(0, 64 * v - B.dhi), cb_hi = min(ncols - 1, 64 * v + 63 - B.dlo);
+    const u64* mask = ws.block_peq + v * kDiagSym;
+    u64 pv = 0, mv = 0;
+    int score = 0;
+    bool started = false;
+    int bottom_min = INT_MAX;  // kDistance, lane 31: minimum of its block's bottom row
+    int in_pack = 0;           // previous step of the lane before: (score << 3) | (processed << 2) | (hout + 1)
     const int src = (lane + 31) & 31;
     for (int t = 0; t <= t_stop; ++t) {
-        int pack[P];
-#pragma unroll
-        for (int j = 0; j < P; ++j) {
-            int c = t - v[j];
-            if (c > cb_hi[j]) {  // the slot's block left the band: its next block
-                v[j] += 32 * P;
-                c -= 32 * P;
-                cb_lo[j] = max(0, 64 * v[j] - B.dhi);
-                cb_hi[j] = min(ncols - 1, 64 * v[j] + 63 - B.dlo);
-                started[j] = false;
-                bottom_min[j] = INT_MAX;
-            }
-            const bool active = v[j] < nb && c >= cb_lo[j] && c <= cb_hi[j];
-            int hout = 0;
-            if (active) {
-                const int up_h = (in_pack[j] & 3) - 1;
-                const bool up_proc = (in_pack[j] >> 2) & 1;
-                const int up_score = in_pack[j] >> 3;
-                const int hin = (v[j] == 0 || !up_proc) ? 1 : up_h;
-                if (!started[j]) {
-                    started[j] = true;
-                    pv[j] = ~0ull;
-                    mv[j] = 0ull;
-                    score[j] = c == 0 ? 64 * (v[j] + 1) : (up_proc ? up_score - up_h : up_score) + 64;
-                }
-                const int tc = io.rev ? io.t[n - 1 - c] : io.t[c];
-                const u64 eq = ws.block_peq[v[j] * kDiagSym + tc];
-                u64 ph;
-                hout = myers_step(pv[j], mv[j], eq, hin, ph);
-                score[j] += hout;
-                if (MODE == kLeaf) {
-                    const int blo = band_lo_block(B, c);
-                    io.leaf[size_t(c) * io.bw + (v[j] - blo)] =
-                        make_uint4(unsigned(pv[j]), unsigned(pv[j] >> 32), unsigned(ph), unsigned(ph >> 32));
-                }
-                if (MODE == kCapture && c == ncols - 1) {
-                    io.cap_pv[v[j]] = pv[j];
-                    io.cap_mv[v[j]] = mv[j];
-                    io.cap_sc[v[j]] = score[j];
-                }
-                if (MODE == kDistance && v[j] == nb - 1 && c == n - 1) {
-                    result = block_value(pv[j], mv[j], score[j], (m - 1) & 63);
-                }
-                if (MODE == kDistance && lane == 31) bottom_min[j] = min(bottom_min[j], score[j]);
-            }
-            pack[j] = (score[j] << 3) | ((active ? 1 : 0) << 2) | (hout + 1);
+        int c = t - v;
+        if (c > cb_hi) {  // the lane's block left the band: its next block
+            v += 32;
+            c -= 32;
+            cb_lo = max(0, 64 * v - B.dhi);
+            cb_hi = min(ncols - 1, 64 * v + 63 - B.dlo);
+            mask = ws.block_peq + v * kDiagSym;
+            started = false;
+            bottom_min = INT_MAX;
         }
-        int recv[P];
-#pragma unroll
-        for (int j = 0; j < P; ++j) recv[j] = __shfl_sync(kFull, pack[j], src);
-        // lane 0's block v - 1 is lane 31's block of the previous group
-#pragma unroll
-        for (int j = 0; j < P; ++j) in_pack[j] = lane == 0 ? recv[(j + P - 1) % P] : recv[j];
+        const bool active = v < nb && c >= cb_lo && c <= cb_hi;
+        int hout = 0;
+        if (active) {
+            const int up_h = (in_pack & 3) - 1;
+            const bool up_proc = (in_pack >> 2) & 1;
+            const int up_score = in_pack >> 3;
+            const int hin = (v == 0 || !up_proc) ? 1 : up_h;
+            if (!started) {
+                started = true;
+                pv = ~0ull;
+                mv = 0ull;
+                score = c == 0 ? 64 * (v + 1) : (up_proc ? up_score - up_h : up_score) + 64;
+            }
+            const int tc = io.rev ? io.t[n - 1 - c] : io.t[c];
+            const u64 eq = mask[tc];
+            u64 ph;
+            hout = myers_step(pv, mv, eq, hin, ph);
+            score += hout;
+            if (MODE == kLeaf) {
+                const int blo = band_lo_block(B, c);
+                io.leaf[size_t(c) * io.bw + (v - blo)] =
+                    make_uint4(unsigned(pv), unsigned(pv >> 32), unsigned(ph), unsigned(ph >> 32));
+            }
+            if (MODE == kCapture && c == ncols - 1) {
+                io.cap_pv[v] = pv;
+                io.cap_mv[v] = mv;
+                io.cap_sc[v] = score;
+            }
+            if (MODE == kDistance && v == nb - 1 && c == n - 1) {
+                result = block_value(pv, mv, score, (m - 1) & 63);
+            }
+            if (MODE == kDistance && lane == 31) bottom_min = min(bottom_min, score);
+        }
+        const int pack = (score << 3) | ((active ? 1 : 0) << 2) | (hout + 1);
+        in_pack = __shfl_sync(kFull, pack, src);
         if (MODE == kDistance && t == chk_t) {
             // the group whose bottom block is chk_v is done (the strip
             // sweep's check after that strip)
             if (chk_v < nb - 1) {
-                int mine = INT_MAX;
-#pragma unroll
-                for (int j = 0; j < P; ++j)
-                    if ((chk_v / 32) % P == j) mine = bottom_min[j];
-                const int row_min = __shfl_sync(kFull, mine, 31);
+                const int row_min = __shfl_sync(kFull, bottom_min, 31);
                 const int R = 64 * chk_v + 63;
                 if (row_min > B.k && R + 1 > B.k) {
                     if (fail) {
@@ -396,14 +369,18 @@ __device__ int warp_sweep_diag(const SweepIO& io, const Band& B, const WarpScrat
     return result;
 }
 
+// Banded block sweep of one subproblem by one warp. MODE kDistance returns
+// the value of cell (m-1, n-1) (INT_MAX if the band never reached it). It
+// also stops early, returning INT_MAX, once every computed cell of a full
+// strip's bottom row R exceeds k and so does the left boundary (R + 1): costs
+// never fall along a path, every path of cost <= k stays inside the band, and
+// a computed in-band value is at most the cost of any path to it inside the
+// band, so no path of cost <= k crosses row R. (Out-of-band cells only lower
+// the minimum.) The distance of a pass that reaches the end is unchanged.
 template <int MODE>
 __device__ int warp_sweep(const SweepIO& io, const Band& B, const WarpScratch& ws, int lane,
                           unsigned int* counters, SweepFail* fail = nullptr) {
-    switch (diag_slots(io, B, ws)) {
-        case 1: return warp_sweep_diag<MODE, 1>(io, B, ws, lane, fail);
-        case 2: return warp_sweep_diag<MODE, 2>(io, B, ws, lane, fail);
-        default: break;
-    }
+    if (diag_sweep_ok(io, B, ws)) return warp_sweep_diag<MODE>(io, B, ws, lane, fail);
     int result = INT_MAX;
     const int nstrips = (B.nb + 31) / 32;
     const int m = B.m, n = B.n;
