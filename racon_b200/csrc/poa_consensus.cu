@@ -272,6 +272,7 @@ __device__ Graph make_graph(const PoaArgs& a, uint32_t slot) {
 struct EndCell {
     int row, value, ties;
     int preds;  // predecessor links over the DP rows (edge-cells = |layer| x (rows + preds))
+    bool h16;   // the layer's score rows in global memory are int16
 };
 
 struct PoaShared {
@@ -1022,9 +1023,37 @@ __device__ EndCell dp_layer(const PoaArgs& a, const Graph& g, const int* order, 
         }
         __syncwarp();
     }
-    // the owner lane of column L holds the end cell
+    // the owner lane of column L holds the end cell (int32 score rows)
     return EndCell{__shfl_sync(kFull, best_r, lane_l), __shfl_sync(kFull, best_v, lane_l),
-                   __shfl_sync(kFull, ties, lane_l), npreds};
+                   __shfl_sync(kFull, ties, lane_l), npreds, false};
+}
+
+// Score rows in global memory (read back for rows beyond the ring and by
+// the walk's re-decisions) are int16 for a layer whose scores provably fit:
+// every score lies between gap x (rows + columns) (the all-gap path, which
+// the maximum includes) and max(match, 0) x columns, so with
+// (ndp + L) x |gap| <= 32767 and max(match, 0) x L <= 32767 no score leaves
+// [-32767, 32767]. Other layers are promoted to int32 rows. Stores saturate,
+// so minus infinity (kNegInf and what is derived from it) becomes -32768,
+// which no score reaches and which reads back as kNegInf. The DP itself
+// stays int32 in registers and in the ring.
+__device__ __forceinline__ bool layer_fits_s16(const PoaArgs& a, int ndp, int L) {
+    return a.gap <= 0 && (long long)(ndp + L) * (long long)(-a.gap) <= 32767 &&
+           (long long)max(int(a.match), 0) * (long long)L <= 32767;
+}
+// two scores in one word, lo in bits 0..15 and hi in bits 16..31, saturated
+__device__ __forceinline__ uint32_t pack_s16(int lo, int hi) {
+    uint32_t d;
+    asm("cvt.pack.sat.s16.s32 %0, %1, %2;" : "=r"(d) : "r"(hi), "r"(lo));
+    return d;
+}
+__device__ __forceinline__ int s16_score(int v) { return v == -32768 ? kNegInf : v; }
+__device__ __forceinline__ int unpack_lo(uint32_t w) { return s16_score(int(w << 16) >> 16); }
+__device__ __forceinline__ int unpack_hi(uint32_t w) { return s16_score(int(w) >> 16); }
+// score (row r, column j) as the layer stored it
+__device__ __forceinline__ int h_at(const Graph& g, int r, int j, bool h16) {
+    if (h16) return s16_score(reinterpret_cast<const int16_t*>(g.H)[r * g.lcap + j]);
+    return g.H[r * g.lcap + j];
 }
 
 // last 512 bytes of each warp's ring hold the 32-row descriptor block
@@ -1046,7 +1075,7 @@ constexpr int kRingDescOffset = (kRingBytesPerWarp - 512) / 16;
 // reads the rest from the row's predecessor count: a single predecessor
 // makes every other cell vertical through it; with several it decides again
 // from H. Requires match >= mismatch and match - mismatch <= 255.
-template <int S>
+template <int S, bool H16>
 __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* order, int ndp, const uint8_t* seq, int L,
                              int lane, int4* ring) {
     static_assert(S % 4 == 0 && S >= 4 && S <= 24, "segment");
@@ -1072,9 +1101,16 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         }
         sc[q] = w;
     }
+    int16_t* const Hs = reinterpret_cast<int16_t*>(g.H);  // the same rows as int16 (H16)
     // row 0 (empty graph prefix) in global memory for the traceback
 #pragma unroll
-    for (int k = 0; k < S; ++k) Hm[j0 + k] = (j0 + k) * gap;
+    for (int k = 0; k < S; ++k) {
+        if (H16) {
+            Hs[j0 + k] = int16_t((j0 + k) * gap);
+        } else {
+            Hm[j0 + k] = (j0 + k) * gap;
+        }
+    }
     const int lane_l = L / S, k_l = L % S;
     int best_v = kNegInf, best_r = INT_MAX, ties = 0, npreds = 0;
     int4* const dblk = ring + kRingDescOffset;
@@ -1128,6 +1164,16 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
                     hv[4 * q + 1] = t4.y;
                     hv[4 * q + 2] = t4.z;
                     hv[4 * q + 3] = t4.w;
+                }
+            } else if (H16) {
+                const uint2* src = reinterpret_cast<const uint2*>(Hs + r * lc + j0);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const uint2 t2 = src[q];
+                    hv[4 * q] = unpack_lo(t2.x);
+                    hv[4 * q + 1] = unpack_hi(t2.x);
+                    hv[4 * q + 2] = unpack_lo(t2.y);
+                    hv[4 * q + 3] = unpack_hi(t2.y);
                 }
             } else {
                 const int4* src = reinterpret_cast<const int4*>(Hm + r * lc + j0);
@@ -1232,11 +1278,17 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         }
         const uint32_t hbit = (hq[0] | hq[1]) | (hq[2] | hq[3]);
         int4* dst_g = reinterpret_cast<int4*>(Hm + i * lc + j0);
+        uint2* dst_s = reinterpret_cast<uint2*>(Hs + i * lc + j0);
         int4* dst_r = ring + (i % R) * Q * 32 + lane;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int4 v4 = make_int4(hv[4 * q], hv[4 * q + 1], hv[4 * q + 2], hv[4 * q + 3]);
-            __stcs(dst_g + q, v4);  // streamed: keep the graph arrays in L2
+            // streamed: keep the graph arrays in L2
+            if (H16) {
+                __stcs(dst_s + q, make_uint2(pack_s16(v4.x, v4.y), pack_s16(v4.z, v4.w)));
+            } else {
+                __stcs(dst_g + q, v4);
+            }
             dst_r[q * 32] = v4;
         }
         __stcs(D2 + bits_at(i, lane), make_uint2(hbit, dbit));
@@ -1257,7 +1309,7 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
     }
     __syncwarp();
     return EndCell{__shfl_sync(kFull, best_r, lane_l), __shfl_sync(kFull, best_v, lane_l),
-                   __shfl_sync(kFull, ties, lane_l), npreds};
+                   __shfl_sync(kFull, ties, lane_l), npreds, H16};
 }
 
 // True when the layer's DP runs in dp_layer_fast (bit-plane decisions).
@@ -1268,13 +1320,23 @@ __device__ __forceinline__ bool fast_dp(const PoaArgs& a, int L) {
 __device__ EndCell dp_dispatch(const PoaArgs& a, const Graph& g, const int* order, int ndp, const uint8_t* seq, int L,
                            int lane, int4* ring) {
     if (fast_dp(a, L)) {
+        if (layer_fits_s16(a, ndp, L)) {
+            switch (seg_cells(L + 1)) {
+                case 4: return dp_layer_fast<4, true>(a, g, order, ndp, seq, L, lane, ring);
+                case 8: return dp_layer_fast<8, true>(a, g, order, ndp, seq, L, lane, ring);
+                case 12: return dp_layer_fast<12, true>(a, g, order, ndp, seq, L, lane, ring);
+                case 16: return dp_layer_fast<16, true>(a, g, order, ndp, seq, L, lane, ring);
+                case 20: return dp_layer_fast<20, true>(a, g, order, ndp, seq, L, lane, ring);
+                default: return dp_layer_fast<24, true>(a, g, order, ndp, seq, L, lane, ring);
+            }
+        }
         switch (seg_cells(L + 1)) {
-            case 4: return dp_layer_fast<4>(a, g, order, ndp, seq, L, lane, ring);
-            case 8: return dp_layer_fast<8>(a, g, order, ndp, seq, L, lane, ring);
-            case 12: return dp_layer_fast<12>(a, g, order, ndp, seq, L, lane, ring);
-            case 16: return dp_layer_fast<16>(a, g, order, ndp, seq, L, lane, ring);
-            case 20: return dp_layer_fast<20>(a, g, order, ndp, seq, L, lane, ring);
-            default: return dp_layer_fast<24>(a, g, order, ndp, seq, L, lane, ring);
+            case 4: return dp_layer_fast<4, false>(a, g, order, ndp, seq, L, lane, ring);
+            case 8: return dp_layer_fast<8, false>(a, g, order, ndp, seq, L, lane, ring);
+            case 12: return dp_layer_fast<12, false>(a, g, order, ndp, seq, L, lane, ring);
+            case 16: return dp_layer_fast<16, false>(a, g, order, ndp, seq, L, lane, ring);
+            case 20: return dp_layer_fast<20, false>(a, g, order, ndp, seq, L, lane, ring);
+            default: return dp_layer_fast<24, false>(a, g, order, ndp, seq, L, lane, ring);
         }
     }
     return dp_layer<24>(a, g, order, ndp, seq, L, lane);
@@ -1890,10 +1952,9 @@ __device__ int heaviest_bundle_warp(const Graph& g, PoaShared& sh, int lane, int
 // else the first whose vertical does, else horizontal. Returns 1000 + p,
 // 2000 + p or 128. Lanes load the candidates of 32 predecessors at a time.
 __device__ uint32_t decide_from_h(const PoaArgs& a, const Graph& g, const int4& d, const uint8_t* seq, int i, int j,
-                                  int lane) {
-    const int lc = g.lcap;
+                                  int lane, bool h16) {
     const int np = desc_np(d.w);
-    const int h = g.H[i * lc + j];
+    const int h = h_at(g, i, j, h16);
     const int s = j > 0 ? (uint32_t(seq[j - 1]) == desc_base(d.w) ? a.match : a.mismatch) : 0;
     const int cnt = np == 0 ? 1 : np;
     int vpick = -1;
@@ -1902,8 +1963,8 @@ __device__ uint32_t decide_from_h(const PoaArgs& a, const Graph& g, const int4& 
         bool dm = false, vm = false;
         if (p < cnt) {
             const int r = desc_pred(g, d, p);
-            dm = j > 0 && g.H[r * lc + j - 1] + s == h;
-            vm = g.H[r * lc + j] + a.gap == h;
+            dm = j > 0 && h_at(g, r, j - 1, h16) + s == h;
+            vm = h_at(g, r, j, h16) + a.gap == h;
         }
         const unsigned bd = __ballot_sync(0xffffffffu, dm);
         if (bd) return 1000u + uint32_t(p0 + __ffs(bd) - 1);
@@ -1923,7 +1984,7 @@ __device__ uint32_t decide_from_h(const PoaArgs& a, const Graph& g, const int4& 
 // predecessor 0; rows of one predecessor are otherwise vertical through it,
 // rows of several decide again from H. Returns false on a broken walk.
 __device__ bool traceback_warp(const PoaArgs& a, const Graph& g, PoaShared& sh, const int* order, const uint8_t* seq,
-                               int L, int iend, int lane, int4* ring) {
+                               int L, int iend, int lane, int4* ring, bool h16) {
     constexpr int W = 64;
     const int S = seg_cells(L + 1);
     int4* const w_desc = ring;                                           // [W]
@@ -1990,7 +2051,7 @@ __device__ bool traceback_warp(const PoaArgs& a, const Graph& g, PoaShared& sh, 
         } else if (np <= 1) {
             code = 64u;  // vertical through the only predecessor
         } else {
-            code = decide_from_h(a, g, d, seq, i, j, lane);
+            code = decide_from_h(a, g, d, seq, i, j, lane, h16);
         }
         if (code < 64u || (code >= 1000u && code < 2000u)) {
             const int p = code < 64u ? int(code) : int(code - 1000u);
@@ -2298,7 +2359,8 @@ __device__ void poa_window(const PoaArgs& a, const Graph& g, PoaShared& sh, uint
             __syncwarp();
         }
         if (fast_dp(a, L)) {
-            if (!sh.fail && !traceback_warp(a, g, sh, order, seq, L, iend, lane, ring) && lane == 0) sh.fail = kFailed;
+            if (!sh.fail && !traceback_warp(a, g, sh, order, seq, L, iend, lane, ring, ec.h16) && lane == 0)
+                sh.fail = kFailed;
         } else if (lane == 0 && !sh.fail && !traceback(a, g, sh, order, seq, L, iend)) {
             sh.fail = kFailed;
         }
