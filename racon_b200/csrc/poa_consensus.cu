@@ -1149,10 +1149,11 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         for (int q = 0; q < Q; ++q) sw[q] = __vcmpeq4(sc[q], cmask) & diff4;
         int T[S];
         uint32_t dbit = 0;
-        auto load_row = [&](int r) {
+        // row r's scores of the lane's segment into dst
+        auto load_row = [&](int r, int (&dst)[S]) {
             if (r == 0) {
 #pragma unroll
-                for (int k = 0; k < S; ++k) hv[k] = (j0 + k) * gap;
+                for (int k = 0; k < S; ++k) dst[k] = (j0 + k) * gap;
             } else if (i - r <= R) {
                 // separate shared and global paths (warp-uniform branch), so
                 // the ring is read with shared-memory loads, not generic ones
@@ -1160,30 +1161,30 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
                     const int4 t4 = src[q * 32];
-                    hv[4 * q] = t4.x;
-                    hv[4 * q + 1] = t4.y;
-                    hv[4 * q + 2] = t4.z;
-                    hv[4 * q + 3] = t4.w;
+                    dst[4 * q] = t4.x;
+                    dst[4 * q + 1] = t4.y;
+                    dst[4 * q + 2] = t4.z;
+                    dst[4 * q + 3] = t4.w;
                 }
             } else if (H16) {
                 const uint2* src = reinterpret_cast<const uint2*>(Hs + r * lc + j0);
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
                     const uint2 t2 = src[q];
-                    hv[4 * q] = unpack_lo(t2.x);
-                    hv[4 * q + 1] = unpack_hi(t2.x);
-                    hv[4 * q + 2] = unpack_lo(t2.y);
-                    hv[4 * q + 3] = unpack_hi(t2.y);
+                    dst[4 * q] = unpack_lo(t2.x);
+                    dst[4 * q + 1] = unpack_hi(t2.x);
+                    dst[4 * q + 2] = unpack_lo(t2.y);
+                    dst[4 * q + 3] = unpack_hi(t2.y);
                 }
             } else {
                 const int4* src = reinterpret_cast<const int4*>(Hm + r * lc + j0);
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
                     const int4 t4 = src[q];
-                    hv[4 * q] = t4.x;
-                    hv[4 * q + 1] = t4.y;
-                    hv[4 * q + 2] = t4.z;
-                    hv[4 * q + 3] = t4.w;
+                    dst[4 * q] = t4.x;
+                    dst[4 * q + 1] = t4.y;
+                    dst[4 * q + 2] = t4.z;
+                    dst[4 * q + 3] = t4.w;
                 }
             }
         };
@@ -1192,11 +1193,37 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
             const int r0 = np == 0 ? 0 : p0;
             int left = left_prev;
             if (r0 != i - 1) {
-                load_row(r0);
+                load_row(r0, hv);
                 left = __shfl_up_sync(kFull, hv[S - 1], 1);
                 if (lane == 0) left = kNegInf;
             }
-            // decision bits gathered in four independent words (short chains)
+            // Several predecessors: the maximum over them of the diagonal
+            // (H[p][j-1] + s) and vertical (H[p][j] + g) terms is the
+            // diagonal and vertical term of their elementwise maximum row M,
+            // so each further row costs one max per cell. hv and left become
+            // M; p0m / p0left mark the columns where the first predecessor
+            // holds M, which is where its diagonal can give T.
+            uint32_t p0m = ~0u;
+            bool p0left = true;
+            for (int p = 1; p < np; ++p) {
+                load_row(np > 3 ? pred_idx[d.x + p] : (p == 1 ? d.y : d.z), T);
+                int lft = __shfl_up_sync(kFull, T[S - 1], 1);
+                if (lane == 0) lft = kNegInf;
+                uint32_t lq[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    bool keep;
+                    hv[k] = __vibmax_s32(hv[k], T[k], &keep);
+                    lq[k & 3] |= uint32_t(!keep) << k;
+                }
+                bool keepl;
+                left = __vibmax_s32(left, lft, &keepl);
+                p0left = p0left && keepl;
+                p0m &= ~((lq[0] | lq[1]) | (lq[2] | lq[3]));
+            }
+            // T = max(M[j-1] + s, M[j] + g); the diagonal of predecessor 0
+            // gives T where it holds M[j-1] and the diagonal is not below the
+            // vertical. Decision bits gathered in four independent words.
             uint32_t dq[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
             for (int k = 0; k < S; ++k) {
@@ -1204,24 +1231,10 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
                 const int dg = pv + mm + sbyte(k);
                 bool dge;
                 T[k] = __vibmax_s32(dg, hv[k] + gap, &dge);
-                dq[k & 3] |= uint32_t(dge) << k;
+                const bool own = k == 0 ? p0left : ((p0m >> (k - 1)) & 1u) != 0u;
+                dq[k & 3] |= uint32_t(dge && own) << k;
             }
             dbit = (dq[0] | dq[1]) | (dq[2] | dq[3]);
-        }
-        for (int p = 1; p < np; ++p) {
-            load_row(np > 3 ? pred_idx[d.x + p] : (p == 1 ? d.y : d.z));
-            int left = __shfl_up_sync(kFull, hv[S - 1], 1);
-            if (lane == 0) left = kNegInf;
-            uint32_t lq[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-            for (int k = 0; k < S; ++k) {
-                const int pv = k == 0 ? left : hv[k - 1];
-                const int mx = __viaddmax_s32(hv[k], gap, pv + mm + sbyte(k));
-                bool keep;
-                T[k] = __vibmax_s32(T[k], mx, &keep);
-                lq[k & 3] |= uint32_t(!keep) << k;
-            }
-            dbit &= ~((lq[0] | lq[1]) | (lq[2] | lq[3]));
         }
         // horizontal term
         constexpr int C = S / 4;  // cells per sub-chain
