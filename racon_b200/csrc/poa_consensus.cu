@@ -1231,10 +1231,9 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
                 const int dg = pv + mm + sbyte(k);
                 bool dge;
                 T[k] = __vibmax_s32(dg, hv[k] + gap, &dge);
-                const bool own = k == 0 ? p0left : ((p0m >> (k - 1)) & 1u) != 0u;
-                dq[k & 3] |= uint32_t(dge && own) << k;
+                dq[k & 3] |= uint32_t(dge) << k;
             }
-            dbit = (dq[0] | dq[1]) | (dq[2] | dq[3]);
+            dbit = ((dq[0] | dq[1]) | (dq[2] | dq[3])) & ((p0m << 1) | (p0left ? 1u : 0u));
         }
         // horizontal term
         constexpr int C = S / 4;  // cells per sub-chain
