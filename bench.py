@@ -50,13 +50,13 @@ sys.path.insert(0, ROOT)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # Thread instructions poa_kernel executes per DP cell, from the same kind of
 # capture (smsp__inst_executed.sum x threads per instruction / DP cells:
-# 6.65 G x 30.28 / 5.84 G)
-POA_THREAD_INST_PER_CELL = 6649564536 * 30.28 / 5838774640
+# 6.33 G x 30.19 / 5.84 G)
+POA_THREAD_INST_PER_CELL = 6329653471 * 30.19 / 5838774640
 # DRAM bytes (read + write) per DP cell of poa_kernel, from one ncu capture of
-# config 1 at 0.1 genome scale (1.411 GB read + 14.983 GB written over
+# config 1 at 0.1 genome scale (1.413 GB read + 14.977 GB written over
 # 5.839 G cells); traffic grows with the cells, so a full launch's traffic is
 # this times its cells
-POA_DRAM_BYTES_PER_CELL = (1.410699e9 + 14.982914e9) / 5838774640
+POA_DRAM_BYTES_PER_CELL = (1.412735e9 + 14.977411e9) / 5838774640
 L2_FLUSH_BYTES = 512 << 20
 # DRAM bytes (read + write) of nw_distance_kernel per nominal cell (query x
 # target span) from one ncu capture of the first 500 pairs of the config-2
