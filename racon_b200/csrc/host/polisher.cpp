@@ -109,12 +109,6 @@ private:
     int pos_ = 0, len_ = 0;
 };
 
-size_t name_end(const std::string& s, size_t from) {
-    size_t e = from;
-    while (e < s.size() && !isspace(uint8_t(s[e]))) ++e;
-    return e;
-}
-
 // Whole file (gzip or plain) in memory; plain files by one fread.
 std::string slurp(const std::string& path, bool& ok) {
     std::string buf;

@@ -68,7 +68,7 @@ struct RingState {
     unsigned long long active_items = 0;
     bool running = false, stopping = false, stopped = false;
     std::string error;
-    uint32_t launches = 0;
+    std::atomic<uint32_t> launches{0};  // read by other threads (stats)
     std::thread thread;
 };
 
@@ -163,7 +163,7 @@ RingService::~RingService() {
 const SvcQueueDev& RingService::queue() const { return st_->q; }
 void* RingService::records() const { return st_->d_recs; }
 size_t RingService::max_batch() const { return size_t(kSvcRing / 2); }
-uint32_t RingService::launches() const { return st_->launches; }
+uint32_t RingService::launches() const { return st_->launches.load(); }
 
 // Keeps the persistent kernel running while items are pending: after the
 // kernel leaves (idle, or racing a publish), items still unclaimed start a
