@@ -1252,15 +1252,19 @@ __device__ EndCell dp_layer_fast(const PoaArgs& a, const Graph& g, const int* or
         int x = agg[0];
 #pragma unroll
         for (int c = 1; c < 4; ++c) x = __viaddmax_s32(x, C * gap, agg[c]);
-        // max-plus prefix of the lane aggregates, x_l = max(x_l, x_(l-1) +
-        // S * gap), one lane per round until no lane changes: monotone and
-        // bounded by the exact prefix, so the fixed point is that prefix.
-        // Horizontal runs rarely cross a whole lane segment, so most rows
-        // take one round instead of the five of a full scan.
-        for (int it = 0; it < 31; ++it) {
-            int y = __shfl_up_sync(kFull, x, 1);
-            if (lane == 0) y = kNegInf;
-            const int nx = __viaddmax_s32(y, S * gap, x);
+        // max-plus prefix of the lane aggregates (penalty S * gap per lane),
+        // rounds of offset 1, 2, 4, 8, 16, stopping at the first round in
+        // which no lane changes: with a uniform penalty per lane, a round of
+        // offset o that changes nothing means x_(l-o) + o S gap <= x_l for
+        // every l, so x_(l-2o) + 2o S gap <= x_(l-o) + o S gap <= x_l and no
+        // later round can change anything either. Horizontal runs rarely
+        // cross a whole lane segment, so most rows stop after one round; a
+        // run across many lanes takes at most five.
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(kFull, x, o);
+            if (lane < o) y = kNegInf;
+            const int nx = __viaddmax_s32(y, o * S * gap, x);
             const bool changed = nx != x;
             x = nx;
             if (!__any_sync(kFull, changed)) break;
